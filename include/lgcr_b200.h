@@ -1,0 +1,220 @@
+/*
+ * lgcr_b200.h — C ABI of the B200-native LGCR Recon implementation.
+ *
+ * This is the drop-in boundary for the `lgcr.Recon` path of
+ * MysteryDove/vapoursynth-LGCR.  Every entry point takes plain pointers,
+ * sizes and strides; no CUDA, VapourSynth or torch types appear in the
+ * signatures (a CUDA stream is passed as `void *`).
+ *
+ * Reference interfaces replaced (paths are within the reference project):
+ *   lgcr_recon_create      <- lgcrCreate            src/plugin.cpp:998-1158
+ *   lgcr_recon_destroy     <- lgcrFree              src/plugin.cpp:992-996
+ *   lgcr_recon_output_format <- viOut query         src/plugin.cpp:1144-1152
+ *   lgcr_recon_frame       <- lgcrGetFrame          src/plugin.cpp:177-721
+ *   lgcr_batch_*           <- frame-parallel getFrame calls (fmParallel,
+ *                             src/plugin.cpp:1157) folded into one launch
+ *   lgcr_server_*          <- the VapourSynth core's concurrent request
+ *                             scheduling of Recon frames (no single
+ *                             reference symbol; see plugin.cpp:215-217
+ *                             for the per-worker workspace pool it sizes)
+ *
+ * Status codes are returned, never traps; error strings mirror the
+ * reference's mapSetError messages where one exists.
+ */
+#ifndef LGCR_B200_H
+#define LGCR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LGCR_B200_VERSION_MAJOR 2
+#define LGCR_B200_VERSION_MINOR 1
+
+/* "argument not given" sentinels (VapourSynth optional arguments) */
+#define LGCR_UNSET_INT (-2147483647 - 1)
+/* doubles: any NaN means "not given" */
+
+/* status codes */
+enum lgcr_status {
+    LGCR_OK = 0,
+    LGCR_E_INVALID = 1,      /* invalid parameter / format (create-time)   */
+    LGCR_E_ARGUMENT = 2,     /* invalid call argument (planes, sizes)      */
+    LGCR_E_CUDA = 3,         /* CUDA runtime error                          */
+    LGCR_E_NOMEM = 4,        /* device or host allocation failed            */
+    LGCR_E_TIMEOUT = 5,      /* bounded wait expired                        */
+    LGCR_E_BUSY = 6,         /* admission refused (budget / queue full)     */
+    LGCR_E_CLOSED = 7,       /* server shut down                            */
+    LGCR_E_INTERNAL = 8
+};
+
+/* colour family values follow VapourSynth API v4 numbering */
+enum { LGCR_CF_GRAY = 1, LGCR_CF_RGB = 2, LGCR_CF_YUV = 3 };
+enum { LGCR_ST_INTEGER = 0, LGCR_ST_FLOAT = 1 };
+/* where frame planes live */
+enum { LGCR_MEM_HOST = 0, LGCR_MEM_DEVICE = 1 };
+
+/* Input clip format (VSVideoInfo subset used by lgcrCreate). */
+typedef struct lgcr_format {
+    int color_family;      /* LGCR_CF_*                                   */
+    int sample_type;       /* LGCR_ST_*                                   */
+    int bits_per_sample;   /* 8..16 integer, 32 float                     */
+    int subsampling_w;     /* log2 horizontal chroma subsampling          */
+    int subsampling_h;     /* log2 vertical chroma subsampling            */
+    int width, height;     /* constant luma dimensions (0 = variable)     */
+} lgcr_format;
+
+/*
+ * Recon arguments, one field per entry of the reference signature
+ *   clip:vnode;width:int:opt;height:int:opt;kernel:data:opt;taps:int:opt;
+ *   algo:int:opt;b:float:opt;c:float:opt;strength:float:opt;sigma:float:opt;
+ *   sratio:float:opt;sdb:float:opt;stretch:float:opt;gsigma:float:opt;
+ *   rescue:float:opt;ridge:int:opt;cedge:int:opt;ar:float:opt;reg:float:opt;
+ *   loc:data:opt;sparse:int:opt;bp:float:opt;ms:float:opt;qgate:float:opt;
+ *   bm:int:opt                                   (src/plugin.cpp:1166-1171)
+ * Ints use LGCR_UNSET_INT, doubles NaN and strings NULL for "not given";
+ * lgcr_params_init() sets every field to "not given".
+ */
+typedef struct lgcr_params {
+    int width, height;
+    const char *kernel;
+    int taps;
+    int algo;
+    double b, c;
+    double strength, sigma, sratio, sdb, stretch, gsigma, rescue;
+    int ridge, cedge;
+    double ar, reg;
+    const char *loc;
+    int sparse;
+    double bp, ms, qgate;
+    int bm;
+} lgcr_params;
+
+/* One plane: pointer, row stride in bytes, dimensions in samples. */
+typedef struct lgcr_plane {
+    void *data;
+    ptrdiff_t stride;
+    int width, height;
+} lgcr_plane;
+
+/* Per-frame work counters (the reference's _LGCR_* profile props,
+ * src/plugin.cpp:126-155). Filled only when requested. */
+typedef struct lgcr_frame_stats {
+    uint64_t output_pixels;
+    uint64_t sparse_active_pixels;   /* trust-mask pixels set            */
+    uint64_t sparse_total_pixels;
+    uint64_t active_output_pixels;   /* guided output pixels             */
+    uint64_t active_chroma_pixels;
+    double sparse_active_ratio;
+    double device_ms;                /* device time of the frame          */
+} lgcr_frame_stats;
+
+typedef struct lgcr_recon lgcr_recon;
+
+void lgcr_params_init(lgcr_params *params);
+
+/* lgcrCreate: validate parameters against the clip format and build the
+ * filter (host weight tables, jinc LUT, device-resident copies).
+ * On failure returns LGCR_E_INVALID and copies the reference's message
+ * into err (if err != NULL). */
+int lgcr_recon_create(const lgcr_params *params, const lgcr_format *fmt,
+                      lgcr_recon **out, char *err, size_t errlen);
+
+/* lgcrFree */
+void lgcr_recon_destroy(lgcr_recon *filter);
+
+/* Output clip format: 4:4:4, same sample type and depth, output size. */
+int lgcr_recon_output_format(const lgcr_recon *filter, lgcr_format *out);
+
+/*
+ * lgcrGetFrame for one frame.
+ *   in[0..2]   Y, U, V source planes (format of create())
+ *   out[0..2]  Y, U, V output planes (4:4:4, output size). When the output
+ *              size equals the input size, out[0].data may be NULL: the
+ *              luma plane is then shared with the input and not written
+ *              (the reference attaches the source luma by reference,
+ *              src/plugin.cpp:265-269).
+ *   chroma_location  the frame's _ChromaLocation (0..5), or -1 if absent.
+ *   memory     LGCR_MEM_HOST: planes are host memory; the call uploads,
+ *              runs and downloads, and returns when the output is written.
+ *              LGCR_MEM_DEVICE: planes are device memory; work is enqueued
+ *              on `stream` (a cudaStream_t, NULL = legacy default stream)
+ *              and the call returns without waiting.
+ *   stats      optional; when non-NULL the call waits for the frame and
+ *              fills the counters.
+ * Safe to call concurrently from several host threads on one filter. */
+int lgcr_recon_frame(lgcr_recon *filter, const lgcr_plane in[3],
+                     const lgcr_plane out[3], int chroma_location,
+                     int memory, void *stream, lgcr_frame_stats *stats);
+
+/* Text of the last error raised on the calling thread. */
+const char *lgcr_last_error(void);
+
+/* ---------------------------------------------------------------------
+ * Batched form: many frames (any mix of filters, sizes, subsamplings and
+ * depths) in one launch per pipeline stage, captured as a CUDA graph and
+ * replayed when the same batch layout is submitted again.
+ * ------------------------------------------------------------------- */
+typedef struct lgcr_batch lgcr_batch;
+
+typedef struct lgcr_batch_item {
+    lgcr_recon *filter;
+    lgcr_plane in[3];        /* device memory */
+    lgcr_plane out[3];       /* device memory */
+    int chroma_location;
+} lgcr_batch_item;
+
+int lgcr_batch_create(lgcr_batch **out);
+void lgcr_batch_destroy(lgcr_batch *batch);
+/* Enqueue all items on `stream`; returns without waiting. use_graph != 0
+ * captures the launch sequence into a CUDA graph on first use of a layout
+ * and replays it afterwards. */
+int lgcr_batch_run(lgcr_batch *batch, const lgcr_batch_item *items, int count,
+                   void *stream, int use_graph);
+/* Number of kernel launches the last lgcr_batch_run enqueued. */
+int lgcr_batch_launch_count(const lgcr_batch *batch);
+
+/* Autotuner: time the candidate launch shapes of every stage on the
+ * given items and keep the fastest per stage (process-wide). */
+int lgcr_autotune(const lgcr_batch_item *items, int count, void *stream,
+                  char *report, size_t reportlen);
+
+/* ---------------------------------------------------------------------
+ * Serving form: a request loop with continuous batching under a device
+ * memory budget. Requests carry host planes; each stream key keeps its
+ * device-resident tables and workspaces.
+ * ------------------------------------------------------------------- */
+typedef struct lgcr_server lgcr_server;
+
+typedef struct lgcr_server_config {
+    size_t device_budget_bytes;   /* admission budget for workspaces      */
+    int max_batch;                /* frames per device batch (>=1)        */
+    int lanes;                    /* concurrent device streams (>=1)      */
+    int queue_capacity;           /* pending requests before LGCR_E_BUSY  */
+} lgcr_server_config;
+
+typedef struct lgcr_request_info {
+    int status;
+    double submit_ms, start_ms, done_ms;   /* server clock, milliseconds */
+    int batch_size;                        /* frames in its device batch  */
+} lgcr_request_info;
+
+int lgcr_server_create(const lgcr_server_config *config, lgcr_server **out);
+/* Submit one frame. Host planes must stay valid until completion.
+ * Returns a ticket (>=0) or a negative status. */
+int64_t lgcr_server_submit(lgcr_server *server, lgcr_recon *filter,
+                           const lgcr_plane in[3], const lgcr_plane out[3],
+                           int chroma_location);
+/* Wait for a ticket (timeout_ms < 0 waits without limit). */
+int lgcr_server_wait(lgcr_server *server, int64_t ticket, int timeout_ms,
+                     lgcr_request_info *info);
+void lgcr_server_destroy(lgcr_server *server);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LGCR_B200_H */

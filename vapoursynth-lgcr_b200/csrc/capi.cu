@@ -1,0 +1,207 @@
+// C ABI of the B200 Recon path (include/lgcr_b200.h): the per-frame drop-in
+// for lgcrGetFrame plus create/destroy/format queries.
+#include "impl.h"
+
+#include <cmath>
+#include <cstring>
+
+using namespace lgcr_b200;
+
+namespace lgcr_b200 {
+const char *lastError();
+}
+
+struct lgcr_recon {
+    Filter *filter;
+};
+
+namespace {
+
+int *zeroPrefix() {
+    static int *buf = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        if (cudaMalloc(&buf, 4096 * sizeof(int)) == cudaSuccess)
+            cudaMemset(buf, 0, 4096 * sizeof(int));
+    });
+    return buf;
+}
+
+cudaStream_t threadStream() {
+    thread_local cudaStream_t s = nullptr;
+    if (!s)
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    return s;
+}
+
+bool checkPlane(const lgcr_plane &p, int w, int h, int bps, bool allowNull) {
+    if (!p.data)
+        return allowNull;
+    return p.width == w && p.height == h && p.stride >= (ptrdiff_t)w * bps;
+}
+
+} // namespace
+
+extern "C" {
+
+void lgcr_params_init(lgcr_params *p) {
+    if (!p)
+        return;
+    p->width = p->height = LGCR_UNSET_INT;
+    p->kernel = nullptr;
+    p->taps = LGCR_UNSET_INT;
+    p->algo = LGCR_UNSET_INT;
+    p->b = p->c = NAN;
+    p->strength = p->sigma = p->sratio = p->sdb = p->stretch = p->gsigma = p->rescue = NAN;
+    p->ridge = p->cedge = LGCR_UNSET_INT;
+    p->ar = p->reg = NAN;
+    p->loc = nullptr;
+    p->sparse = LGCR_UNSET_INT;
+    p->bp = p->ms = p->qgate = NAN;
+    p->bm = LGCR_UNSET_INT;
+}
+
+const char *lgcr_last_error(void) { return lastError(); }
+
+int lgcr_recon_create(const lgcr_params *params, const lgcr_format *fmt, lgcr_recon **out,
+                      char *err, size_t errlen) {
+    std::string msg;
+    Filter *f = nullptr;
+    const int status = createFilter(params, fmt, &f, msg);
+    if (status != LGCR_OK) {
+        setError(msg);
+        if (err && errlen) {
+            std::strncpy(err, msg.c_str(), errlen - 1);
+            err[errlen - 1] = '\0';
+        }
+        return status;
+    }
+    *out = new lgcr_recon{f};
+    return LGCR_OK;
+}
+
+void lgcr_recon_destroy(lgcr_recon *h) {
+    if (!h)
+        return;
+    cudaDeviceSynchronize();
+    delete h->filter;
+    delete h;
+}
+
+int lgcr_recon_output_format(const lgcr_recon *h, lgcr_format *out) {
+    if (!h || !out)
+        return LGCR_E_ARGUMENT;
+    *out = h->filter->fmt;
+    out->subsampling_w = out->subsampling_h = 0;
+    out->width = h->filter->p.outW;
+    out->height = h->filter->p.outH;
+    return LGCR_OK;
+}
+
+int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out[3],
+                     int chroma_location, int memory, void *stream, lgcr_frame_stats *stats) {
+    if (!h || !in || !out) {
+        setError("LGCR: null argument");
+        return LGCR_E_ARGUMENT;
+    }
+    Filter &F = *h->filter;
+    const int bps = F.bytesPerSample();
+    const bool sameSize = F.p.outW == F.sw && F.p.outH == F.sh;
+    if (!checkPlane(in[0], F.sw, F.sh, bps, false) || !checkPlane(in[1], F.cw, F.ch, bps, false) ||
+        !checkPlane(in[2], F.cw, F.ch, bps, false) ||
+        !checkPlane(out[0], F.p.outW, F.p.outH, bps, sameSize) ||
+        !checkPlane(out[1], F.p.outW, F.p.outH, bps, false) ||
+        !checkPlane(out[2], F.p.outW, F.p.outH, bps, false)) {
+        setError("LGCR: plane dimensions or strides do not match the clip format");
+        return LGCR_E_ARGUMENT;
+    }
+    if (memory != LGCR_MEM_HOST && memory != LGCR_MEM_DEVICE) {
+        setError("LGCR: memory must be LGCR_MEM_HOST or LGCR_MEM_DEVICE");
+        return LGCR_E_ARGUMENT;
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : (memory == LGCR_MEM_HOST ? threadStream() : nullptr);
+    FrameTask t;
+    t.filter = &F;
+    t.p = F.sited(chroma_location);
+    t.tables = F.tablesFor(t.p.shiftX, t.p.shiftY);
+    if (!t.tables) {
+        setError("LGCR: failed to upload geometry tables");
+        return LGCR_E_NOMEM;
+    }
+    Workspace *ws = F.acquire();
+    if (!ws) {
+        setError("LGCR: device workspace allocation failed");
+        return LGCR_E_NOMEM;
+    }
+    // the pinned job slot is rewritten below: the previous frame that used
+    // this workspace must have consumed it
+    if (ws->used)
+        cudaEventSynchronize(ws->done);
+    t.ws = ws;
+    cudaError_t e = cudaSuccess;
+    if (memory == LGCR_MEM_HOST) {
+        for (int i = 0; i < 3; ++i) {
+            e = cudaMemcpy2DAsync(ws->stageIn[i], ws->stageInPitch[i], in[i].data, in[i].stride,
+                                  size_t(in[i].width) * bps, in[i].height, cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) break;
+            t.in[i] = { ws->stageIn[i], (ptrdiff_t)ws->stageInPitch[i], in[i].width, in[i].height };
+            t.out[i] = { ws->stageOut[i], (ptrdiff_t)ws->stageOutPitch[i], F.p.outW, F.p.outH };
+        }
+        if (!out[0].data)
+            t.out[0].data = nullptr;
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            t.in[i] = in[i];
+            t.out[i] = out[i];
+        }
+    }
+    if (e == cudaSuccess) {
+        buildJob(t, *ws->hJob);
+        e = cudaMemcpyAsync(ws->dJob, ws->hJob, sizeof(FrameJob), cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess) {
+        std::vector<FrameJob> jobs(1, *ws->hJob);
+        StagePlan plan;
+        planStages(jobs, plan);
+        if (launchStages(jobs, plan, ws->dJob, zeroPrefix(), s) < 0)
+            e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && memory == LGCR_MEM_HOST) {
+        for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+            if (!out[i].data)
+                continue;
+            e = cudaMemcpy2DAsync(out[i].data, out[i].stride, ws->stageOut[i], ws->stageOutPitch[i],
+                                  size_t(F.p.outW) * bps, F.p.outH, cudaMemcpyDeviceToHost, s);
+        }
+    }
+    unsigned long long counters[kCntCount] = {};
+    if (e == cudaSuccess && stats)
+        e = cudaMemcpyAsync(counters, ws->counters, sizeof(counters), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(ws->done, s);
+    ws->used = true;
+    const FrameJob J = *ws->hJob;
+    F.release(ws);
+    if (e == cudaSuccess && (memory == LGCR_MEM_HOST || stats))
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return cudaFail(e, "lgcr_recon_frame");
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->output_pixels = uint64_t(J.W) * J.H;
+        if (J.sparse) {
+            stats->sparse_active_pixels = counters[kCntMaskPixels];
+            stats->sparse_total_pixels = uint64_t(J.sw) * J.sh;
+            stats->active_output_pixels = counters[kCntActiveOutput];
+            stats->active_chroma_pixels = counters[kCntActiveChroma];
+            stats->sparse_active_ratio = double(counters[kCntMaskPixels]) / (double(J.sw) * J.sh);
+        } else {
+            stats->active_output_pixels = stats->output_pixels;
+            stats->active_chroma_pixels = uint64_t(J.cw) * J.ch;
+            stats->sparse_active_ratio = 1.0;
+        }
+    }
+    return LGCR_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,160 @@
+// Host runtime of the B200 Recon path: filters, resident tables, device
+// workspaces and the stage scheduler shared by the per-frame, batched and
+// serving forms.
+#pragma once
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lgcr_b200.h"
+#include "geometry.h"
+#include "recon.cuh"
+
+namespace lgcr_b200 {
+
+// Resolved Recon arguments (the reference's LGCRData, src/lgcr.h:123-164).
+struct FilterParams {
+    int outW = 0, outH = 0;
+    KernelSpec k;
+    int taps = 6;
+    double strength = 0.8, sigma = 0.01, sratio = 0.15, sdb = 3.0, reg = 0.005;
+    double stretch = 1.0, gsigma = 2.5, rescue = 1.0;
+    int algo = 2;
+    bool ridge = true, cedge = false;
+    double ms = 1.0, qgate = 1.0;
+    bool sparse = true, locSet = false, bm = false;
+    double bp = 0.0, arMargin = 0.0;
+    double shiftX = -0.5, shiftY = 0.0;
+};
+
+// A device allocation carved into 256-byte aligned pieces.
+class DeviceArena {
+public:
+    DeviceArena() = default;
+    ~DeviceArena();
+    DeviceArena(const DeviceArena &) = delete;
+    DeviceArena &operator=(const DeviceArena &) = delete;
+    // two-phase use: reserve() sizes, commit() allocates, then take() again
+    size_t reserve(size_t bytes) { const size_t o = size_; size_ += (bytes + 255) & ~size_t(255); return o; }
+    bool commit();
+    void *at(size_t offset) const { return static_cast<char *>(base_) + offset; }
+    size_t size() const { return size_; }
+private:
+    void *base_ = nullptr;
+    size_t size_ = 0;
+};
+
+// Geometry tables of one (filter, chroma siting), resident in HBM.
+struct DeviceTables {
+    double shiftX = 0, shiftY = 0;
+    DeviceArena arena;
+    AxisView ax{}, ay{};
+    RadialView rad{};
+    WeightView lumaH{}, lumaV{};
+    const int *lcXb = nullptr, *lcXe = nullptr, *lcYb = nullptr, *lcYe = nullptr;
+    // algo 6
+    WeightView ycH1{}, ycV1{}, ycH2{}, ycV2{};
+    AxisView sax{}, say{};
+    RadialView srad{};
+    int nyqX = 0, nyqY = 0;
+    // algo 4
+    const int *lsX = nullptr, *lsY = nullptr;
+    const float *lsXf = nullptr, *lsYf = nullptr;
+    // bm
+    const int *bmStartsX = nullptr, *bmStartsY = nullptr;
+    int bmAnchorsX = 0, bmAnchorsY = 0;
+    int axSup = 0, aySup = 0;
+};
+
+struct Filter;
+
+// Per-frame device workspace (planes sized for the filter's geometry).
+struct Workspace {
+    Filter *owner = nullptr;
+    DeviceArena arena;
+    FrameJob *dJob = nullptr;           // device slot for the per-frame form
+    FrameJob *hJob = nullptr;           // pinned host staging of the job
+    float *Yw = nullptr, *Uw = nullptr, *Vw = nullptr;
+    float *jxx = nullptr, *jxy = nullptr, *jyy = nullptr, *lc = nullptr, *ms = nullptr;
+    uint8_t *seed = nullptr, *mtmp = nullptr, *mask = nullptr, *cmask = nullptr;
+    float *oU = nullptr, *oV = nullptr, *lumaTmp = nullptr;
+    unsigned long long *counters = nullptr;
+    float *aff = nullptr, *yc1 = nullptr, *yc2 = nullptr, *ycTmp = nullptr;
+    float *detail = nullptr, *detailTmp = nullptr, *detailTmp2 = nullptr;
+    float *lgf = nullptr, *selW2 = nullptr, *selW3 = nullptr, *gU = nullptr, *gV = nullptr;
+    uint8_t *roi = nullptr;
+    float *bmAcc = nullptr, *bmGuide = nullptr, *bmPatch = nullptr;
+    int *bmGroups = nullptr;
+    void *stageIn[3] = {nullptr, nullptr, nullptr};
+    void *stageOut[3] = {nullptr, nullptr, nullptr};
+    size_t stageInPitch[3] = {0, 0, 0}, stageOutPitch[3] = {0, 0, 0};
+    cudaEvent_t done = nullptr;
+    bool used = false;
+    ~Workspace();
+};
+
+struct FrameTask {
+    Filter *filter = nullptr;
+    Workspace *ws = nullptr;
+    const DeviceTables *tables = nullptr;
+    FilterParams p;                     // with the frame's siting applied
+    lgcr_plane in[3], out[3];           // device planes
+};
+
+struct Filter {
+    FilterParams p;
+    lgcr_format fmt{};
+    int sw = 0, sh = 0, cw = 0, ch = 0;
+    float *dLut = nullptr;
+    std::mutex mu;
+    std::vector<std::unique_ptr<DeviceTables>> tables;
+    std::vector<std::unique_ptr<Workspace>> idle;
+    std::atomic<int> live{0};
+    ~Filter();
+
+    const DeviceTables *tablesFor(double shiftX, double shiftY);
+    Workspace *acquire();
+    void release(Workspace *ws);
+    std::unique_ptr<Workspace> makeWorkspace(bool hostStaging);
+    size_t workspaceBytes();
+    FilterParams sited(int chromaLocation) const;
+    bool isFloat() const { return fmt.sample_type == LGCR_ST_FLOAT; }
+    int bytesPerSample() const { return isFloat() ? 4 : (fmt.bits_per_sample > 8 ? 2 : 1); }
+    bool directOutput(const FilterParams &q) const;
+    bool needsBackProjection(const FilterParams &q) const;
+};
+
+// Creates a Filter from Recon arguments; mirrors lgcrCreate's validation.
+int createFilter(const lgcr_params *params, const lgcr_format *fmt, Filter **out,
+                 std::string &err);
+
+// Fill the device FrameJob of one task.
+void buildJob(const FrameTask &t, FrameJob &job);
+
+// Stage scheduler: launches every stage once over all jobs. `dJobs` is the
+// device copy of `jobs`; `dPrefix` receives the stage prefix tables (space
+// for stageCount * (n + 1) ints) and is written from `hPrefix` (pinned,
+// same size) by one copy. Returns the number of kernel launches, or -1.
+struct StagePlan {
+    std::vector<int> prefix;            // stageCount * (n+1)
+    std::vector<int> totals;            // blocks per stage
+    int maxDil = 0;
+    int nyqPasses = 0;
+};
+int stageCount();
+void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan);
+int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan,
+                 const FrameJob *dJobs, const int *dPrefix, cudaStream_t stream);
+
+const char *setError(const std::string &msg);
+int cudaFail(cudaError_t e, const char *where);
+
+} // namespace lgcr_b200

@@ -1,0 +1,51 @@
+// Kernel declarations of the Recon path. Every kernel takes
+// (jobs, tileStart, njobs): FrameJob array, per-stage block prefix table,
+// number of frames in the launch.
+#pragma once
+
+#include "recon.cuh"
+
+namespace lgcr_b200 {
+
+#define LGCR_STAGE_ARGS const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs
+
+__global__ void k_convert(LGCR_STAGE_ARGS);
+__global__ void k_tensor(LGCR_STAGE_ARGS);
+__global__ void k_lc(LGCR_STAGE_ARGS);
+__global__ void k_dilate_h(LGCR_STAGE_ARGS);
+__global__ void k_dilate_v(LGCR_STAGE_ARGS);
+__global__ void k_mark_chroma(LGCR_STAGE_ARGS);
+__global__ void k_count(LGCR_STAGE_ARGS);
+__global__ void k_gate(LGCR_STAGE_ARGS);
+__global__ void k_recon(LGCR_STAGE_ARGS);
+__global__ void k_luma_h(LGCR_STAGE_ARGS);
+__global__ void k_luma_v(LGCR_STAGE_ARGS);
+__global__ void k_luma_radial(LGCR_STAGE_ARGS);
+__global__ void k_store_chroma(LGCR_STAGE_ARGS);
+// algo 6
+__global__ void k_yc_h(LGCR_STAGE_ARGS);
+__global__ void k_affine(LGCR_STAGE_ARGS);
+__global__ void k_detail_plain(LGCR_STAGE_ARGS);
+__global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass);
+__global__ void k_detail_resize_h(LGCR_STAGE_ARGS);
+__global__ void k_detail_resize_v(LGCR_STAGE_ARGS);
+__global__ void k_detail_resize_radial(LGCR_STAGE_ARGS);
+__global__ void k_detail_transfer(LGCR_STAGE_ARGS);
+// algo 4
+__global__ void k_lgf(LGCR_STAGE_ARGS);
+__global__ void k_roi(LGCR_STAGE_ARGS);
+__global__ void k_blend(LGCR_STAGE_ARGS);
+// bm / bp
+__global__ void k_bm_guide(LGCR_STAGE_ARGS);
+__global__ void k_bm_group(LGCR_STAGE_ARGS);
+__global__ void k_bm_aggregate(LGCR_STAGE_ARGS);
+__global__ void k_backproject(LGCR_STAGE_ARGS);
+
+// Tile helpers shared by the 32x8 per-pixel stages.
+__device__ __forceinline__ void tile32x8(int tile, int width, int &x, int &y) {
+    const int tilesX = (width + 31) / 32;
+    x = (tile % tilesX) * 32 + threadIdx.x;
+    y = (tile / tilesX) * 8 + threadIdx.y;
+}
+
+} // namespace lgcr_b200

@@ -1,0 +1,463 @@
+// algo 6 (constrained detail transfer) and algo 4 (selector) stages.
+//   k_yc              buildYcFilteredMaps + median3 consensus    src/maps.cpp:529-680,
+//                                                                src/algos.cpp:813-815
+//   k_affine          buildAffineMaps: 5x5 hull + 16 moments     src/algos.cpp:1026-1137,
+//                     (sparse: direct sums, *1/n; dense: /n)     src/algos.cpp:1382-1526
+//   k_detail_plain    plain reconstruct of D(Y) minus Y          src/algos.cpp:1528-1585
+//   k_detail_nyq      dyadic [1/4,1/2,1/4] Nyquist passes        src/algos.cpp:1139-1364
+//   k_detail_resize_* detail to output size                      src/algos.cpp:1366-1380
+//   k_detail_transfer detailTransferImpl                         src/algos.cpp:1587-1698
+//   k_lgf             buildLGFPair moments + ms fade             src/algos.cpp:300-448,
+//                                                                src/plugin.cpp:418-425,543-551
+//   k_roi             selector ROI marking                       src/plugin.cpp:496-531
+//   k_blend           blendSelector / blendSelectorCompressed    src/algos.cpp:453-593
+// Window moments are FP64 sums of exact float products in raster order.
+#include "kernels.cuh"
+#include "plain.cuh"
+
+namespace lgcr_b200 {
+
+__device__ __forceinline__ float median3f(float a, float b, float c) {
+    const float mn = smin(smin(a, b), c);
+    const float mx = smax(smax(a, b), c);
+    return a + b + c - mn - mx;
+}
+
+// separable candidate D(Y) at one chroma sample: H pass (double acc, float
+// store) on each needed luma row, then V pass (double acc).
+__device__ __forceinline__ float candidateAt(const FrameJob &J, const WeightView &th,
+                                             const WeightView &tv, int cx, int cy) {
+    const int sv = __ldg(tv.start + cy);
+    const float *wv = tv.w + (size_t)cy * tv.sup;
+    const int shs = __ldg(th.start + cx);
+    const float *wh = th.w + (size_t)cx * th.sup;
+    double acc = 0.0;
+    for (int j = 0; j < tv.sup; ++j) {
+        const float *row = J.Y + (size_t)iclamp(sv + j, 0, J.sh - 1) * J.sw;
+        double hv = 0.0;
+        for (int i = 0; i < th.sup; ++i)
+            hv = fma((double)__ldg(wh + i), (double)ldf(row + iclamp(shs + i, 0, J.sw - 1)), hv);
+        acc = fma((double)__ldg(wv + j), (double)(float)hv, acc);
+    }
+    return (float)acc;
+}
+
+__global__ void k_yc_h(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int cx, cy;
+    tile32x8(blockIdx.x - tileStart[f], J.cw, cx, cy);
+    if (cx >= J.cw || cy >= J.ch)
+        return;
+    const size_t o = (size_t)cy * J.cw + cx;
+    const float y1 = candidateAt(J, J.ycH1, J.ycV1, cx, cy);
+    const float y2 = candidateAt(J, J.ycH2, J.ycV2, cx, cy);
+    J.yc1[o] = y1;
+    J.yc2[o] = y2;
+    const size_t C = (size_t)J.cw * J.ch;
+    J.aff[8 * C + o] = median3f(ldf(J.lc + o), y1, y2);   // degraded luma consensus
+}
+
+// 5x5 affine statistics per chroma sample (active samples when sparse).
+__global__ void __launch_bounds__(256)
+k_affine(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
+    const int w = J.cw, h = J.ch;
+    if (x >= w || y >= h)
+        return;
+    const size_t o = (size_t)y * w + x;
+    const bool sparseRoi = J.sparse &&
+        (unsigned long long)J.counters[kCntActiveChroma] * 2ull < (unsigned long long)w * h;
+    if (sparseRoi && J.cmask[o] == 0)
+        return;
+    const int top = max(0, y - 2), bottom = min(h - 1, y + 2);
+    const int left = max(0, x - 2), right = min(w - 1, x + 2);
+    const float *yc[3] = { J.lc, J.yc1, J.yc2 };
+    double s[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s[k] = 0.0;
+    float mnU = ldf(J.U + (size_t)top * w + left), mxU = mnU;
+    float mnV = ldf(J.V + (size_t)top * w + left), mxV = mnV;
+    for (int py = top; py <= bottom; ++py)
+        for (int px = left; px <= right; ++px) {
+            const size_t q = (size_t)py * w + px;
+            const float uf = ldf(J.U + q), vf = ldf(J.V + q);
+            const double u = uf, v = vf;
+            s[0] += u; s[1] += u * u; s[2] += v; s[3] += v * v;
+            mnU = smin(mnU, uf); mxU = smax(mxU, uf);
+            mnV = smin(mnV, vf); mxV = smax(mxV, vf);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double ly = ldf(yc[k] + q);
+                const int b = 4 + 4 * k;
+                s[b] += ly; s[b + 1] += ly * ly; s[b + 2] += ly * u; s[b + 3] += ly * v;
+            }
+        }
+    const int n = (right - left + 1) * (bottom - top + 1);
+    const double eps = J.lgfEps;
+    const double epsSig = J.epsSig;
+    const double inv = 1.0 / n;
+    auto mean = [&](double sum) { return sparseRoi ? sum * inv : sum / n; };
+    const double meanU = mean(s[0]), meanV = mean(s[2]);
+    const double varU = smax(0.0, mean(s[1]) - meanU * meanU);
+    const double varV = smax(0.0, mean(s[3]) - meanV * meanV);
+    double q[3], aU[3], aV[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int b = 4 + 4 * k;
+        const double meanY = mean(s[b]);
+        const double varY = smax(0.0, mean(s[b + 1]) - meanY * meanY);
+        const double covU = mean(s[b + 2]) - meanY * meanU;
+        const double covV = mean(s[b + 3]) - meanY * meanV;
+        aU[k] = sclamp(covU / (varY + eps), -16.0, 16.0);
+        aV[k] = sclamp(covV / (varY + eps), -16.0, 16.0);
+        q[k] = sclamp((covU * covU + covV * covV) / ((varY + eps) * (varU + varV + eps)), 0.0, 1.0);
+    }
+    const size_t C = (size_t)w * h;
+    float *A = J.aff;
+    A[0 * C + o] = median3f((float)aU[0], (float)aU[1], (float)aU[2]);
+    A[1 * C + o] = median3f((float)aV[0], (float)aV[1], (float)aV[2]);
+    const double qmax = smax(smax(q[0], q[1]), q[2]);
+    const double qmin = smin(smin(q[0], q[1]), q[2]);
+    const double stability = qmax > 1e-9 ? qmin / qmax : 0.0;
+    const double chromaSignal = (varU + varV) / (varU + varV + epsSig);
+    A[2 * C + o] = (float)(((q[0] + q[1] + q[2]) / 3.0) * stability * chromaSignal);
+    A[3 * C + o] = mnU;
+    A[4 * C + o] = mxU;
+    A[5 * C + o] = mnV;
+    A[6 * C + o] = mxV;
+    A[7 * C + o] = smax(mxU - mnU, mxV - mnV);
+}
+
+// detail = Y - plain(D(Y)) on the source luma grid.
+__global__ void k_detail_plain(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.sw, x, y);
+    if (x >= J.sw || y >= J.sh)
+        return;
+    PlainCtx c = chromaPlainCtx(J);
+    c.p0 = J.aff + 8 * (size_t)J.cw * J.ch;
+    c.p1 = nullptr;
+    c.ax = J.sax;
+    c.ay = J.say;
+    c.rad = J.srad;
+    c.invWxC = J.sinvWxC;
+    c.invWyC = J.sinvWyC;
+    float r, unused;
+    plainAt(c, x, y, r, unused);
+    const size_t o = (size_t)y * J.sw + x;
+    J.detailTmp[o] = ldf(J.Y + o) - r;
+}
+
+// One dyadic pass: x passes (steps 1,2,4..) then y passes; ping-pong
+// between detailTmp and detailTmp2.
+__global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.sw, x, y);
+    if (x >= J.sw || y >= J.sh)
+        return;
+    const float *src = (pass & 1) ? J.detailTmp2 : J.detailTmp;
+    float *dst = (pass & 1) ? J.detailTmp : J.detailTmp2;
+    const int w = J.sw, h = J.sh;
+    float a, b, c;
+    if (pass < J.nyqX) {
+        const int step = 1 << pass;
+        const float *row = src + (size_t)y * w;
+        a = row[max(0, x - step)]; b = row[x]; c = row[min(w - 1, x + step)];
+    } else {
+        const int step = 1 << (pass - J.nyqX);
+        a = src[(size_t)max(0, y - step) * w + x];
+        b = src[(size_t)y * w + x];
+        c = src[(size_t)min(h - 1, y + step) * w + x];
+    }
+    dst[(size_t)y * w + x] = 0.25f * a + 0.5f * b + 0.25f * c;
+}
+
+__global__ void k_detail_resize_h(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.W, x, y);
+    if (x >= J.W || y >= J.sh)
+        return;
+    const WeightView &t = J.lumaH;
+    const int s = __ldg(t.start + x);
+    const float *wp = t.w + (size_t)x * t.sup;
+    const float *row = J.detailSrc + (size_t)y * J.sw;
+    double acc = 0.0;
+    for (int j = 0; j < t.sup; ++j)
+        acc = fma((double)__ldg(wp + j), (double)row[iclamp(s + j, 0, J.sw - 1)], acc);
+    J.lumaTmp[(size_t)y * J.W + x] = (float)acc;
+}
+
+__global__ void k_detail_resize_v(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.W, x, y);
+    if (x >= J.W || y >= J.H)
+        return;
+    const WeightView &t = J.lumaV;
+    const int s = __ldg(t.start + y);
+    const float *wp = t.w + (size_t)y * t.sup;
+    double acc = 0.0;
+    for (int j = 0; j < t.sup; ++j)
+        acc = fma((double)__ldg(wp + j),
+                  (double)J.lumaTmp[(size_t)iclamp(s + j, 0, J.sh - 1) * J.W + x], acc);
+    J.detail[(size_t)y * J.W + x] = (float)acc;
+}
+
+__global__ void k_detail_resize_radial(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H)
+        return;
+    const double sx = (double)J.sw / J.W, sy = (double)J.sh / J.H;
+    const double widen = fmax(1.0, fmax(sx, sy));
+    const float invW = (float)(1.0 / widen);
+    const int radius = (int)ceil(J.support * widen);
+    const int sup = 2 * radius;
+    const double cy = (oy + 0.5) * sy - 0.5;
+    const int y0 = (int)ceil(cy - radius);
+    const double cx = (ox + 0.5) * sx - 0.5;
+    const int x0 = (int)ceil(cx - radius);
+    double acc = 0.0, wsum = 0.0;
+    for (int j = 0; j < sup; ++j) {
+        const int ty = iclamp(y0 + j, 0, J.sh - 1);
+        const float dy = (float)((y0 + j - cy) * invW);
+        const float *row = J.detailSrc + (size_t)ty * J.sw;
+        for (int i = 0; i < sup; ++i) {
+            const int tx = iclamp(x0 + i, 0, J.sw - 1);
+            const float dx = (float)((x0 + i - cx) * invW);
+            const float w = lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
+            acc = fma((double)w, (double)row[tx], acc);
+            wsum += (double)w;
+        }
+    }
+    J.detail[(size_t)oy * J.W + ox] = (float)(wsum > 1e-6 ? acc / wsum : 0.0);
+}
+
+__device__ __forceinline__ bool activeOut(const FrameJob &J, int ox, int oy) {
+    if (!J.sparse)
+        return true;
+    const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
+    const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
+    return J.mask[(size_t)my * J.sw + mx] != 0;
+}
+
+__global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
+        return;
+    const AxisView &ax = J.ax, &ay = J.ay;
+    const int lxi = __ldg(ax.lbI0 + ox), lyi = __ldg(ay.lbI0 + oy);
+    const float lxf = __ldg(ax.lbF + ox), lyf = __ldg(ay.lbF + oy);
+    const float jxx = bilinearFast(J.jxx, J.sw, J.sh, lxi, lxf, lyi, lyf);
+    const float jxy = bilinearFast(J.jxy, J.sw, J.sh, lxi, lxf, lyi, lyf);
+    const float jyy = bilinearFast(J.jyy, J.sw, J.sh, lxi, lxf, lyi, lyf);
+    const TensorDir dir = principalDirection(jxx, jxy, jyy);
+    const int cxi = __ldg(ax.cbI0 + ox), cyi = __ldg(ay.cbI0 + oy);
+    const float cxf = __ldg(ax.cbF + ox), cyf = __ldg(ay.cbF + oy);
+    const int cw = J.cw, ch = J.ch;
+    const size_t C = (size_t)cw * ch;
+    const float q = bilinearFast(J.aff + 2 * C, cw, ch, cxi, cxf, cyi, cyf);
+    float g = (1.0f - J.qgate * (1.0f - q)) * J.strength;
+    if (J.useMs) {
+        const float ms = bilinearFast(J.ms, cw, ch, cxi, cxf, cyi, cyf);
+        g *= 1.0f - J.msStrength * (1.0f - ms);
+    }
+    const float au = bilinearFast(J.aff + 0 * C, cw, ch, cxi, cxf, cyi, cyf);
+    const float av = bilinearFast(J.aff + 1 * C, cw, ch, cxi, cxf, cyi, cyf);
+    const float coherence = dir.coherence;
+    const float tx = -dir.ny, ty = dir.nx;
+    const float *dl = J.detail;
+    const float dc = dl[(size_t)oy * J.W + ox];
+    const float s = 1.0f + J.stretch * coherence;
+    const float dtp = bilinearAt(dl, J.W, J.H, (float)ox + tx * s, (float)oy + ty * s);
+    const float dtm = bilinearAt(dl, J.W, J.H, (float)ox - tx * s, (float)oy - ty * s);
+    const float dt = 0.25f * dtp + 0.5f * dc + 0.25f * dtm;
+    const float det = dc + (dt - dc) * coherence;
+    const float cap = 0.5f * bilinearFast(J.aff + 7 * C, cw, ch, cxi, cxf, cyi, cyf);
+    const float cu = sclamp(g * au * det, -cap, cap);
+    const float cv = sclamp(g * av * det, -cap, cap);
+    const size_t o = (size_t)oy * J.W + ox;
+    const float ru = J.oU[o], rv = J.oV[o];
+    float ou = ru + cu, ov = rv + cv;
+    if (J.clampHull) {
+        const float ar = J.margin;
+        const float loU = smin(ru, bilinearFast(J.aff + 3 * C, cw, ch, cxi, cxf, cyi, cyf) - ar);
+        const float hiU = smax(ru, bilinearFast(J.aff + 4 * C, cw, ch, cxi, cxf, cyi, cyf) + ar);
+        const float loV = smin(rv, bilinearFast(J.aff + 5 * C, cw, ch, cxi, cxf, cyi, cyf) - ar);
+        const float hiV = smax(rv, bilinearFast(J.aff + 6 * C, cw, ch, cxi, cxf, cyi, cyf) + ar);
+        ou = sclamp(ou, loU, hiU);
+        ov = sclamp(ov, loV, hiV);
+    }
+    J.oU[o] = ou;
+    J.oV[o] = ov;
+}
+
+// ---------------------------------------------------------------------------
+// algo 4
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float pointLuma(const FrameJob &J, int x, int y) {
+    return bilinearFast(J.Y, J.sw, J.sh, __ldg(J.lsX + x), __ldg(J.lsXf + x),
+                        __ldg(J.lsY + y), __ldg(J.lsYf + y));
+}
+
+// LGF regression per chroma sample: 5x5 sums of {l, l^2, u, l*u, v, l*v}
+// with l the point-sampled luma; conf = var/(var+eps) (x cedge fade), then
+// the mutual-structure fade. Integer output: all samples; float: ROI only.
+__global__ void __launch_bounds__(256)
+k_lgf(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
+    const int w = J.cw, h = J.ch;
+    if (x >= w || y >= h)
+        return;
+    const size_t o = (size_t)y * w + x;
+    if (J.lgfRoiOnly && J.roi[o] == 0)
+        return;
+    const int top = max(0, y - 2), bottom = min(h - 1, y + 2);
+    const int left = max(0, x - 2), right = min(w - 1, x + 2);
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int py = top; py <= bottom; ++py)
+        for (int px = left; px <= right; ++px) {
+            const double ly = pointLuma(J, px, py);
+            const double u = ldf(J.U + (size_t)py * w + px), v = ldf(J.V + (size_t)py * w + px);
+            s[0] += ly; s[1] += ly * ly; s[2] += u; s[3] += ly * u; s[4] += v; s[5] += ly * v;
+        }
+    const int n = (right - left + 1) * (bottom - top + 1);
+    const double eps = J.lgfEps;
+    const double meanY = s[0] / n;
+    const double var = s[1] / n - meanY * meanY;
+    const double meanU = s[2] / n, meanV = s[4] / n;
+    const double slopeU = (s[3] / n - meanY * meanU) / (var + eps);
+    const double slopeV = (s[5] / n - meanY * meanV) / (var + eps);
+    const size_t C = (size_t)w * h;
+    float *L = J.lgf;
+    L[0 * C + o] = (float)slopeU;
+    L[1 * C + o] = (float)(meanU - slopeU * meanY);
+    L[3 * C + o] = (float)slopeV;
+    L[4 * C + o] = (float)(meanV - slopeV * meanY);
+    const float base = (float)(var / (var + eps));
+    float confU = base, confV = base;
+    if (J.cedge) {
+        auto lsAt = [&](int xx, int yy) { return pointLuma(J, iclamp(xx, 0, w - 1), iclamp(yy, 0, h - 1)); };
+        const float lgx = (lsAt(x + 1, y) - lsAt(x - 1, y)) * 0.5f;
+        const float lgy = (lsAt(x, y + 1) - lsAt(x, y - 1)) * 0.5f;
+        const float gl = hypotf(lgx, lgy);
+        auto fade = [&](const float *P) {
+            float mn = P[(size_t)max(0, y - 2) * w + max(0, x - 2)], mx = mn;
+            for (int py = y - 2; py <= y + 2; ++py)
+                for (int px = x - 2; px <= x + 2; ++px) {
+                    const float v = P[(size_t)iclamp(py, 0, h - 1) * w + iclamp(px, 0, w - 1)];
+                    mn = smin(mn, v); mx = smax(mx, v);
+                }
+            const float range = mx - mn;
+            if (gl <= 1e-9f || range <= 1e-6f)
+                return 1.0f;
+            auto at = [&](int xx, int yy) { return P[(size_t)iclamp(yy, 0, h - 1) * w + iclamp(xx, 0, w - 1)]; };
+            const float cgx = (at(x + 1, y) - at(x - 1, y)) * 0.5f;
+            const float cgy = (at(x, y + 1) - at(x, y - 1)) * 0.5f;
+            const float gradN = fabsf(cgx * lgx / gl + cgy * lgy / gl);
+            const float width = range / (gradN + 1e-6f);
+            return sclamp((2.2f - width) / 0.7f, 0.0f, 1.0f);
+        };
+        confU *= fade(J.U);
+        confV *= fade(J.V);
+    }
+    if (J.useMs) {
+        const float fm = 1.0f - J.msStrength * (1.0f - J.ms[o]);
+        confU *= fm;
+        confV *= fm;
+    }
+    L[2 * C + o] = confU;
+    L[5 * C + o] = confV;
+}
+
+// Mark the 2x2 chroma footprint of output samples whose diagonal routing
+// weight reaches 1e-4.
+__global__ void k_roi(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
+        return;
+    if (J.selW3[(size_t)oy * J.W + ox] < 1e-4f)
+        return;
+    const int cx0 = __ldg(J.ax.cbI0 + ox), cx1 = min(cx0 + 1, J.cw - 1);
+    const int cy0 = __ldg(J.ay.cbI0 + oy), cy1 = min(cy0 + 1, J.ch - 1);
+    J.roi[(size_t)cy0 * J.cw + cx0] = 1;
+    J.roi[(size_t)cy0 * J.cw + cx1] = 1;
+    J.roi[(size_t)cy1 * J.cw + cx0] = 1;
+    J.roi[(size_t)cy1 * J.cw + cx1] = 1;
+}
+
+__global__ void k_blend(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
+        return;
+    const size_t o = (size_t)oy * J.W + ox;
+    const float lam = J.strength4;
+    const bool compressed = J.sparse &&
+        (unsigned long long)J.counters[kCntActiveOutput] * 2ull < (unsigned long long)J.W * J.H;
+    const int cw = J.cw, ch = J.ch;
+    const size_t C = (size_t)cw * ch;
+    const int cx = __ldg(J.ax.cbI0 + ox), cy = __ldg(J.ay.cbI0 + oy);
+    const float cxf = __ldg(J.ax.cbF + ox), cyf = __ldg(J.ay.cbF + oy);
+    const float plainU = J.oU[o], plainV = J.oV[o];
+    if (compressed) {
+        const float w3 = lam * J.selW3[o];
+        float valueU = plainU + lam * J.gU[o];
+        float valueV = plainV + lam * J.gV[o];
+        if (w3 != 0.0f) {
+            const float luma = bilinearFast(J.Y, J.sw, J.sh, __ldg(J.ax.lbI0 + ox), __ldg(J.ax.lbF + ox),
+                                            __ldg(J.ay.lbI0 + oy), __ldg(J.ay.lbF + oy));
+            const float au = bilinearFast(J.lgf + 0 * C, cw, ch, cx, cxf, cy, cyf);
+            const float bu = bilinearFast(J.lgf + 1 * C, cw, ch, cx, cxf, cy, cyf);
+            const float cu = bilinearFast(J.lgf + 2 * C, cw, ch, cx, cxf, cy, cyf);
+            const float av = bilinearFast(J.lgf + 3 * C, cw, ch, cx, cxf, cy, cyf);
+            const float bv = bilinearFast(J.lgf + 4 * C, cw, ch, cx, cxf, cy, cyf);
+            const float cv = bilinearFast(J.lgf + 5 * C, cw, ch, cx, cxf, cy, cyf);
+            valueU += w3 * cu * (au * luma + bu - plainU);
+            valueV += w3 * cv * (av * luma + bv - plainV);
+        }
+        J.oU[o] = valueU;
+        J.oV[o] = valueV;
+        return;
+    }
+    const float w2v = J.selW2[o] * lam;
+    const float w3v = J.selW3[o] * lam;
+    if (w2v < 1e-4f && w3v < 1e-4f)
+        return;
+    const float L0 = bilinearFast(J.Y, J.sw, J.sh, __ldg(J.ax.lbI0 + ox), __ldg(J.ax.lbF + ox),
+                                  __ldg(J.ay.lbI0 + oy), __ldg(J.ay.lbF + oy));
+    const float au = bilinearFast(J.lgf + 0 * C, cw, ch, cx, cxf, cy, cyf);
+    const float bu = bilinearFast(J.lgf + 1 * C, cw, ch, cx, cxf, cy, cyf);
+    const float cu = bilinearFast(J.lgf + 2 * C, cw, ch, cx, cxf, cy, cyf);
+    const float av = bilinearFast(J.lgf + 3 * C, cw, ch, cx, cxf, cy, cyf);
+    const float bv = bilinearFast(J.lgf + 4 * C, cw, ch, cx, cxf, cy, cyf);
+    const float cv = bilinearFast(J.lgf + 5 * C, cw, ch, cx, cxf, cy, cyf);
+    J.oU[o] = plainU + (w2v * (J.gU[o] - plainU) + w3v * cu * (au * L0 + bu - plainU));
+    J.oV[o] = plainV + (w2v * (J.gV[o] - plainV) + w3v * cv * (av * L0 + bv - plainV));
+}
+
+} // namespace lgcr_b200

@@ -1,0 +1,714 @@
+// Host runtime: filter creation (lgcrCreate, src/plugin.cpp:998-1158),
+// per-siting resident tables, workspaces and the stage scheduler that
+// replaces lgcrGetFrame's sequence of stage calls (src/plugin.cpp:177-721)
+// with one launch per stage covering every frame of a batch.
+#include "impl.h"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace lgcr_b200 {
+
+static thread_local std::string tlsError;
+
+const char *setError(const std::string &msg) {
+    tlsError = msg;
+    return tlsError.c_str();
+}
+
+const char *lastError() { return tlsError.c_str(); }
+
+int cudaFail(cudaError_t e, const char *where) {
+    setError(std::string("LGCR: CUDA error in ") + where + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? LGCR_E_NOMEM : LGCR_E_CUDA;
+}
+
+DeviceArena::~DeviceArena() {
+    if (base_)
+        cudaFree(base_);
+}
+
+bool DeviceArena::commit() {
+    if (base_ || size_ == 0)
+        return true;
+    return cudaMalloc(&base_, size_) == cudaSuccess;
+}
+
+Workspace::~Workspace() {
+    if (done)
+        cudaEventDestroy(done);
+    if (hJob)
+        cudaFreeHost(hJob);
+}
+
+Filter::~Filter() {
+    if (dLut)
+        cudaFree(dLut);
+}
+
+// ---------------------------------------------------------------------------
+// lgcrCreate
+// ---------------------------------------------------------------------------
+static bool given(int v) { return v != LGCR_UNSET_INT; }
+static bool given(double v) { return !std::isnan(v); }
+
+int createFilter(const lgcr_params *pp, const lgcr_format *fmt, Filter **out, std::string &err) {
+    auto fail = [&](const char *msg) { err = msg; return LGCR_E_INVALID; };
+    if (!pp || !fmt || !out)
+        return fail("LGCR: null argument");
+    const lgcr_params &a = *pp;
+    const bool isFloat = fmt->sample_type == LGCR_ST_FLOAT;
+    if (fmt->color_family != LGCR_CF_YUV || (isFloat && fmt->bits_per_sample != 32) ||
+        (!isFloat && (fmt->bits_per_sample < 8 || fmt->bits_per_sample > 16)) ||
+        (fmt->sample_type != LGCR_ST_FLOAT && fmt->sample_type != LGCR_ST_INTEGER))
+        return fail("LGCR: input must be planar YUV (8-16 bit int or 32 bit float)");
+    if (fmt->subsampling_w > 1 || fmt->subsampling_h > 1 || fmt->subsampling_w < 0 ||
+        fmt->subsampling_h < 0)
+        return fail("LGCR: only 4:4:4 / 4:2:2 / 4:2:0 input is supported");
+    if (fmt->width <= 0 || fmt->height <= 0)
+        return fail("LGCR: constant input dimensions required");
+
+    auto f = std::make_unique<Filter>();
+    FilterParams &d = f->p;
+    f->fmt = *fmt;
+    d.outW = given(a.width) ? a.width : fmt->width;
+    d.outH = given(a.height) ? a.height : fmt->height;
+    if (d.outW <= 0 || d.outH <= 0)
+        return fail("LGCR: invalid width/height");
+
+    const std::string k = a.kernel ? a.kernel : "lanczos";
+    KernelSpec &ks = d.k;
+    if (k == "bilinear") {
+        ks.kernel = Kernel::Bilinear;
+        ks.support = 1.0;
+    } else if (k == "bicubic") {
+        ks.kernel = Kernel::Bicubic;
+        ks.support = 2.0;
+        ks.kp1 = given(a.b) ? a.b : 0.0;
+        ks.kp2 = given(a.c) ? a.c : 0.6;
+    } else if (k == "lanczos") {
+        ks.kernel = Kernel::Lanczos;
+        const long taps = given(a.taps) ? a.taps : 3;
+        if (taps < 1 || taps > 64)
+            return fail("LGCR: lanczos taps must be in the range 1..64");
+        ks.kp1 = double(taps);
+        ks.support = ks.kp1;
+    } else if (k == "spline16") {
+        ks.kernel = Kernel::Spline16;
+        ks.support = 2.0;
+    } else if (k == "spline36") {
+        ks.kernel = Kernel::Spline36;
+        ks.support = 3.0;
+    } else if (k == "jinc") {
+        ks.kernel = Kernel::Jinc;
+        ks.radial = true;
+        const long taps = given(a.taps) ? a.taps : 3;
+        if (taps < 1 || taps > 64)
+            return fail("LGCR: jinc taps must be in the range 1..64");
+        ks.kp1 = double(taps);
+        ks.support = ks.kp1;
+        const int n = static_cast<int>(ks.support * 1024) + 2;
+        ks.lut.resize(n);
+        for (int i = 0; i < n; ++i)
+            ks.lut[i] = static_cast<float>(jincWindowed(double(i) / 1024.0, ks.support));
+        ks.lutScale = 1024.0f;
+    } else {
+        return fail("LGCR: kernel must be \"bilinear\", \"bicubic\", \"lanczos\", \"spline16\", "
+                    "\"spline36\" or \"jinc\"");
+    }
+    d.taps = 2 * static_cast<int>(std::ceil(ks.support));
+    d.strength = given(a.strength) ? a.strength : 0.8;
+    d.sigma = given(a.sigma) ? a.sigma : 0.01;
+    d.sratio = given(a.sratio) ? a.sratio : 0.15;
+    d.algo = given(a.algo) ? a.algo : 2;
+    if (d.algo != 2 && d.algo != 4 && d.algo != 6)
+        return fail("LGCR: algo must be 2 (guided), 4 (selector) or 6 (detail transfer)");
+    d.sdb = given(a.sdb) ? a.sdb : 3.0;
+    d.stretch = given(a.stretch) ? a.stretch : 1.0;
+    d.gsigma = given(a.gsigma) ? a.gsigma : 2.5;
+    d.rescue = given(a.rescue) ? a.rescue : 1.0;
+    d.ridge = given(a.ridge) ? (a.ridge != 0) : true;
+    d.cedge = given(a.cedge) ? (a.cedge != 0) : false;
+    d.ms = given(a.ms) ? a.ms : 1.0;
+    d.qgate = given(a.qgate) ? a.qgate : 1.0;
+    d.arMargin = given(a.ar) ? a.ar : 0.0;
+    d.reg = given(a.reg) ? a.reg : 0.005;
+    if (a.loc) {
+        const std::string l = a.loc;
+        if (l == "left") d.shiftX = -0.5;
+        else if (l == "center") d.shiftX = 0.0;
+        else return fail("LGCR: loc must be \"left\" or \"center\"");
+        d.locSet = true;
+    } else {
+        d.shiftX = -0.5;
+    }
+    d.sparse = given(a.sparse) ? (a.sparse != 0) : true;
+    d.bm = given(a.bm) ? (a.bm != 0) : false;
+    d.bp = given(a.bp) ? a.bp : 0.0;
+    if (fmt->subsampling_w == 0)
+        d.shiftX = 0.0;
+    if (fmt->subsampling_h == 0)
+        d.shiftY = 0.0;
+    if (d.strength < 0.0 || d.strength > 1.0 || d.sigma <= 0.0 || d.sratio <= 0.0 ||
+        d.sdb <= 0.0 || d.stretch < 0.0 || d.gsigma <= 0.0 || d.reg <= 0.0 ||
+        d.bp < 0.0 || d.bp > 1.0 || d.ms < 0.0 || d.ms > 1.0 ||
+        d.qgate < 0.0 || d.qgate > 1.0 || d.rescue < 0.0 || d.rescue > 1.0)
+        return fail("LGCR: invalid parameter range (need 0<=strength/rescue<=1, 0<=bp/ms/qgate<=1, "
+                    "sigma/sratio/sdb/gsigma/reg>0, stretch>=0)");
+
+    f->sw = fmt->width;
+    f->sh = fmt->height;
+    f->cw = (fmt->width + (1 << fmt->subsampling_w) - 1) >> fmt->subsampling_w;
+    f->ch = (fmt->height + (1 << fmt->subsampling_h) - 1) >> fmt->subsampling_h;
+    if (!ks.lut.empty()) {
+        cudaError_t e = cudaMalloc(&f->dLut, ks.lut.size() * sizeof(float));
+        if (e != cudaSuccess) { err = std::string("LGCR: ") + cudaGetErrorString(e); return LGCR_E_NOMEM; }
+        e = cudaMemcpy(f->dLut, ks.lut.data(), ks.lut.size() * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { err = std::string("LGCR: ") + cudaGetErrorString(e); return LGCR_E_CUDA; }
+    }
+    *out = f.release();
+    return LGCR_OK;
+}
+
+// applyFrameChromaSiting, src/plugin.cpp:157-175
+FilterParams Filter::sited(int cl) const {
+    FilterParams q = p;
+    if (fmt.subsampling_w == 0) q.shiftX = 0.0;
+    if (fmt.subsampling_h == 0) q.shiftY = 0.0;
+    if (q.locSet || cl < 0)
+        return q;
+    if (fmt.subsampling_w > 0)
+        q.shiftX = (cl == 0 || cl == 2 || cl == 4) ? -0.5 : 0.0;
+    if (fmt.subsampling_h > 0)
+        q.shiftY = (cl == 2 || cl == 3) ? -0.5 : (cl == 4 || cl == 5) ? 0.5 : 0.0;
+    return q;
+}
+
+bool Filter::needsBackProjection(const FilterParams &q) const {
+    return q.bp > 0.0 && q.outW == sw && q.outH == sh && cw * 2 == sw && ch * 2 == sh;
+}
+
+bool Filter::directOutput(const FilterParams &q) const {
+    if (q.bm || needsBackProjection(q))
+        return false;
+    return q.strength == 0.0 || q.algo == 2 || (q.algo == 4 && !isFloat());
+}
+
+// ---------------------------------------------------------------------------
+// resident tables
+// ---------------------------------------------------------------------------
+namespace {
+
+// Host image of a table arena: arrays are appended with their offsets.
+struct Packer {
+    std::vector<uint8_t> bytes;
+    template <class T> size_t add(const std::vector<T> &v) {
+        const size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + v.size() * sizeof(T));
+        if (!v.empty())
+            std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+struct AxisOffsets { size_t start, w, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF; int n, sup; };
+
+AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
+    AxisOffsets o;
+    o.n = a.n; o.sup = a.sup;
+    o.start = pk.add(a.start); o.w = pk.add(a.w); o.am = pk.add(a.am);
+    o.wsum = pk.add(a.weightSum); o.wabs = pk.add(a.absoluteWeightSum);
+    o.pos = pk.add(a.pos); o.lpos = pk.add(a.lpos);
+    o.cbI0 = pk.add(a.chromaBilin.i0); o.cbF = pk.add(a.chromaBilin.f);
+    o.lbI0 = pk.add(a.lumaBilin.i0); o.lbF = pk.add(a.lumaBilin.f);
+    return o;
+}
+
+AxisView axisView(const DeviceArena &ar, const AxisOffsets &o) {
+    AxisView v;
+    v.n = o.n; v.sup = o.sup;
+    v.start = (const int *)ar.at(o.start); v.w = (const float *)ar.at(o.w);
+    v.am = (const uint8_t *)ar.at(o.am); v.wsum = (const float *)ar.at(o.wsum);
+    v.wabs = (const float *)ar.at(o.wabs); v.pos = (const float *)ar.at(o.pos);
+    v.lpos = (const float *)ar.at(o.lpos); v.cbI0 = (const int *)ar.at(o.cbI0);
+    v.cbF = (const float *)ar.at(o.cbF); v.lbI0 = (const int *)ar.at(o.lbI0);
+    v.lbF = (const float *)ar.at(o.lbF);
+    return v;
+}
+
+struct WeightOffsets { size_t start, w; int n, sup; };
+WeightOffsets packWeights(Packer &pk, const WeightTable &t) {
+    return { pk.add(t.start), pk.add(t.w), t.n, t.sup };
+}
+WeightView weightView(const DeviceArena &ar, const WeightOffsets &o) {
+    return { o.n, o.sup, (const int *)ar.at(o.start), (const float *)ar.at(o.w) };
+}
+
+struct RadialOffsets { size_t xPhase, yPhase, weights; int valid, supX, supY, phasesX; };
+RadialOffsets packRadial(Packer &pk, const RadialTable &t) {
+    RadialOffsets o{};
+    o.valid = t.valid;
+    o.supX = t.supportX; o.supY = t.supportY; o.phasesX = t.phaseCountX;
+    if (t.valid) {
+        o.xPhase = pk.add(t.xPhase); o.yPhase = pk.add(t.yPhase); o.weights = pk.add(t.weights);
+    }
+    return o;
+}
+RadialView radialView(const DeviceArena &ar, const RadialOffsets &o) {
+    RadialView v{};
+    v.valid = o.valid;
+    v.supX = o.supX; v.supY = o.supY; v.phasesX = o.phasesX;
+    if (o.valid) {
+        v.xPhase = (const uint16_t *)ar.at(o.xPhase);
+        v.yPhase = (const uint16_t *)ar.at(o.yPhase);
+        v.weights = (const float *)ar.at(o.weights);
+    }
+    return v;
+}
+
+} // namespace
+
+const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &t : tables)
+        if (t->shiftX == shiftX && t->shiftY == shiftY)
+            return t.get();
+    auto t = std::make_unique<DeviceTables>();
+    t->shiftX = shiftX;
+    t->shiftY = shiftY;
+    const double rw = double(sw) / cw, rh = double(sh) / ch;
+    const ChromaAxis ax = buildChromaAxis(sw, p.outW, rw, shiftX, p.k);
+    const ChromaAxis ay = buildChromaAxis(sh, p.outH, rh, shiftY, p.k);
+    Packer pk;
+    const AxisOffsets oax = packAxis(pk, ax), oay = packAxis(pk, ay);
+    RadialOffsets orad{};
+    if (p.k.radial)
+        orad = packRadial(pk, buildRadialTable(p.k, ax, ay, cw, ch));
+    const bool sameSize = p.outW == sw && p.outH == sh;
+    WeightOffsets olh{}, olv{};
+    if (!sameSize && !p.k.radial) {
+        olh = packWeights(pk, buildWeights(sw, p.outW, p.k, 0.0));
+        olv = packWeights(pk, buildWeights(sh, p.outH, p.k, 0.0));
+    }
+    // algo 6: degradation candidates, source-grid plain axes, Nyquist levels
+    const bool algo6 = p.algo == 6 && p.strength > 0.0;
+    WeightOffsets oy1h{}, oy1v{}, oy2h{}, oy2v{};
+    AxisOffsets osax{}, osay{};
+    RadialOffsets osrad{};
+    if (algo6) {
+        KernelSpec bil;
+        bil.kernel = Kernel::Bilinear; bil.kp1 = bil.kp2 = 0.0; bil.support = 1.0;
+        KernelSpec bic;
+        bic.kernel = Kernel::Bicubic; bic.kp1 = 0.0; bic.kp2 = 0.6; bic.support = 2.0;
+        oy1h = packWeights(pk, buildWeights(sw, cw, bil, shiftX));
+        oy1v = packWeights(pk, buildWeights(sh, ch, bil, shiftY));
+        oy2h = packWeights(pk, buildWeights(sw, cw, bic, shiftX));
+        oy2v = packWeights(pk, buildWeights(sh, ch, bic, shiftY));
+        const ChromaAxis sax = buildChromaAxis(sw, sw, rw, shiftX, p.k);
+        const ChromaAxis say = buildChromaAxis(sh, sh, rh, shiftY, p.k);
+        osax = packAxis(pk, sax);
+        osay = packAxis(pk, say);
+        if (p.k.radial)
+            osrad = packRadial(pk, buildRadialTable(p.k, sax, say, cw, ch));
+    }
+    // algo 4: point-sampled luma positions (pointSampledLuma, algos.cpp:300-315)
+    const bool algo4 = p.algo == 4 && p.strength > 0.0;
+    size_t olsX = 0, olsXf = 0, olsY = 0, olsYf = 0;
+    if (algo4) {
+        std::vector<float> xPos(cw), yPos(ch);
+        for (int x = 0; x < cw; ++x)
+            xPos[x] = float((x + 0.5) * rw - 0.5 + shiftX);
+        for (int y = 0; y < ch; ++y)
+            yPos[y] = float((y + 0.5) * rh - 0.5 + shiftY);
+        const BilinAxis bx = buildBilinAxis(xPos, sw), by = buildBilinAxis(yPos, sh);
+        olsX = pk.add(bx.i0); olsXf = pk.add(bx.f);
+        olsY = pk.add(by.i0); olsYf = pk.add(by.f);
+    }
+    std::vector<int> xb, xe, yb, ye;
+    lcExtents(sw, cw, rw, shiftX, xb, xe);
+    lcExtents(sh, ch, rh, shiftY, yb, ye);
+    const size_t oxb = pk.add(xb), oxe = pk.add(xe), oyb = pk.add(yb), oye = pk.add(ye);
+
+    t->arena.reserve(pk.bytes.size());
+    if (!t->arena.commit())
+        return nullptr;
+    if (cudaMemcpy(t->arena.at(0), pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+        return nullptr;
+    t->ax = axisView(t->arena, oax);
+    t->ay = axisView(t->arena, oay);
+    t->axSup = ax.sup;
+    t->aySup = ay.sup;
+    if (p.k.radial)
+        t->rad = radialView(t->arena, orad);
+    if (!sameSize && !p.k.radial) {
+        t->lumaH = weightView(t->arena, olh);
+        t->lumaV = weightView(t->arena, olv);
+    }
+    if (algo6) {
+        t->ycH1 = weightView(t->arena, oy1h);
+        t->ycV1 = weightView(t->arena, oy1v);
+        t->ycH2 = weightView(t->arena, oy2h);
+        t->ycV2 = weightView(t->arena, oy2v);
+        t->sax = axisView(t->arena, osax);
+        t->say = axisView(t->arena, osay);
+        if (p.k.radial)
+            t->srad = radialView(t->arena, osrad);
+        auto levels = [](double ratio) {
+            int n = 0;
+            while (ratio > 1.5 && n < 4) { ratio *= 0.5; ++n; }
+            return n;
+        };
+        t->nyqX = levels(rw);
+        t->nyqY = levels(rh);
+    }
+    if (algo4) {
+        t->lsX = (const int *)t->arena.at(olsX);
+        t->lsXf = (const float *)t->arena.at(olsXf);
+        t->lsY = (const int *)t->arena.at(olsY);
+        t->lsYf = (const float *)t->arena.at(olsYf);
+    }
+    t->lcXb = (const int *)t->arena.at(oxb);
+    t->lcXe = (const int *)t->arena.at(oxe);
+    t->lcYb = (const int *)t->arena.at(oyb);
+    t->lcYe = (const int *)t->arena.at(oye);
+    tables.push_back(std::move(t));
+    return tables.back().get();
+}
+
+// ---------------------------------------------------------------------------
+// workspaces
+// ---------------------------------------------------------------------------
+std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
+    auto ws = std::make_unique<Workspace>();
+    ws->owner = this;
+    DeviceArena &ar = ws->arena;
+    const size_t L = size_t(sw) * sh, C = size_t(cw) * ch, O = size_t(p.outW) * p.outH;
+    const bool guided = p.strength > 0.0;
+    const bool sameSize = p.outW == sw && p.outH == sh;
+    const int bps = bytesPerSample();
+    struct Slot { size_t off = 0; bool on = false; };
+    auto take = [&](size_t bytes, bool on = true) { Slot s; s.on = on; if (on) s.off = ar.reserve(bytes); return s; };
+    Slot sJob = take(sizeof(FrameJob));
+    Slot sY = take(L * 4), sU = take(C * 4), sV = take(C * 4);
+    Slot sJxx = take(L * 4, guided), sJxy = take(L * 4, guided), sJyy = take(L * 4, guided);
+    Slot sLc = take(C * 4, guided), sMs = take(C * 4, guided && p.ms > 0.0);
+    const bool sparse = guided && p.sparse;
+    Slot sSeed = take(L, sparse), sMtmp = take(L, sparse), sMask = take(L, sparse), sCmask = take(C, sparse);
+    Slot sOU = take(O * 4), sOV = take(O * 4);
+    Slot sLumaTmp = take(size_t(p.outW) * sh * 4, !sameSize && !p.k.radial);  // luma / detail resize
+    Slot sCnt = take(kCntCount * sizeof(unsigned long long));
+    const bool algo6 = guided && p.algo == 6, algo4 = guided && p.algo == 4;
+    Slot sAff = take(9 * C * 4, algo6), sYc1 = take(C * 4, algo6), sYc2 = take(C * 4, algo6);
+    Slot sDt1 = take(L * 4, algo6), sDt2 = take(L * 4, algo6);
+    Slot sDet = take(O * 4, algo6 && !sameSize);
+    Slot sLumaTmp2 = take(size_t(p.outW) * sh * 4, algo6 && !sameSize && !p.k.radial && false);
+    Slot sLgf = take(6 * C * 4, algo4);
+    const bool sel = algo4 && isFloat();
+    Slot sW2 = take(O * 4, sel), sW3 = take(O * 4, sel), sGU = take(O * 4, sel), sGV = take(O * 4, sel);
+    Slot sRoi = take(C, sel);
+    Slot sIn[3], sOut[3];
+    for (int i = 0; i < 3; ++i) {
+        const size_t n = i == 0 ? L : C;
+        sIn[i] = take(n * bps, hostStaging);
+        sOut[i] = take(O * bps, hostStaging);
+    }
+    if (!ar.commit())
+        return nullptr;
+    auto F = [&](const Slot &s) { return s.on ? (float *)ar.at(s.off) : nullptr; };
+    auto B = [&](const Slot &s) { return s.on ? (uint8_t *)ar.at(s.off) : nullptr; };
+    ws->dJob = (FrameJob *)ar.at(sJob.off);
+    ws->Yw = F(sY); ws->Uw = F(sU); ws->Vw = F(sV);
+    ws->jxx = F(sJxx); ws->jxy = F(sJxy); ws->jyy = F(sJyy);
+    ws->lc = F(sLc); ws->ms = F(sMs);
+    ws->seed = B(sSeed); ws->mtmp = B(sMtmp); ws->mask = B(sMask); ws->cmask = B(sCmask);
+    ws->oU = F(sOU); ws->oV = F(sOV); ws->lumaTmp = F(sLumaTmp);
+    ws->counters = (unsigned long long *)ar.at(sCnt.off);
+    ws->aff = F(sAff); ws->yc1 = F(sYc1); ws->yc2 = F(sYc2);
+    ws->detailTmp = F(sDt1); ws->detailTmp2 = F(sDt2); ws->detail = F(sDet);
+    (void)sLumaTmp2;
+    ws->lgf = F(sLgf);
+    ws->selW2 = F(sW2); ws->selW3 = F(sW3); ws->gU = F(sGU); ws->gV = F(sGV);
+    ws->roi = B(sRoi);
+    for (int i = 0; i < 3; ++i) {
+        const int w = i == 0 ? sw : cw;
+        ws->stageIn[i] = sIn[i].on ? ar.at(sIn[i].off) : nullptr;
+        ws->stageInPitch[i] = size_t(w) * bps;
+        ws->stageOut[i] = sOut[i].on ? ar.at(sOut[i].off) : nullptr;
+        ws->stageOutPitch[i] = size_t(p.outW) * bps;
+    }
+    if (cudaEventCreateWithFlags(&ws->done, cudaEventDisableTiming) != cudaSuccess)
+        return nullptr;
+    if (cudaHostAlloc((void **)&ws->hJob, sizeof(FrameJob), cudaHostAllocDefault) != cudaSuccess)
+        return nullptr;
+    return ws;
+}
+
+// Prefer an idle workspace whose last frame has finished on the device; grow
+// the pool (up to a few per filter) rather than wait for one in flight.
+Workspace *Filter::acquire() {
+    constexpr int kMaxWorkspaces = 4;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (size_t i = 0; i < idle.size(); ++i) {
+            Workspace *ws = idle[i].get();
+            if (!ws->used || cudaEventQuery(ws->done) == cudaSuccess) {
+                idle[i].release();
+                idle.erase(idle.begin() + i);
+                return ws;
+            }
+        }
+        if (live.load() >= kMaxWorkspaces && !idle.empty()) {
+            Workspace *ws = idle.front().release();
+            idle.erase(idle.begin());
+            return ws;   // caller waits for its event
+        }
+    }
+    auto ws = makeWorkspace(true);
+    if (ws)
+        live.fetch_add(1);
+    return ws.release();
+}
+
+void Filter::release(Workspace *ws) {
+    if (!ws)
+        return;
+    std::lock_guard<std::mutex> lock(mu);
+    idle.emplace_back(ws);
+}
+
+// ---------------------------------------------------------------------------
+// FrameJob
+// ---------------------------------------------------------------------------
+static int sampleKind(const lgcr_format &f) {
+    if (f.sample_type == LGCR_ST_FLOAT) return kF32;
+    return f.bits_per_sample > 8 ? kU16 : kU8;
+}
+
+void buildJob(const FrameTask &t, FrameJob &J) {
+    std::memset(&J, 0, sizeof(J));
+    const Filter &F = *t.filter;
+    const FilterParams &p = t.p;
+    const DeviceTables &T = *t.tables;
+    Workspace &ws = *t.ws;
+    J.sw = F.sw; J.sh = F.sh; J.cw = F.cw; J.ch = F.ch; J.W = p.outW; J.H = p.outH;
+    J.rw = double(F.sw) / F.cw;
+    J.rh = double(F.sh) / F.ch;
+    J.rwF = float(J.rw);
+    J.rhF = float(J.rh);
+    J.sameSize = (J.W == J.sw && J.H == J.sh);
+    J.inKind = J.outKind = sampleKind(F.fmt);
+    J.bits = F.fmt.bits_per_sample;
+    const bool isFloat = F.isFloat();
+    J.yScale = isFloat ? 1.0 : 1.0 / double((1 << J.bits) - 1);
+    J.cOffset = isFloat ? 0.0 : -0.5;
+    const double outScale = isFloat ? 1.0 : double((1 << J.bits) - 1);
+    J.qScale = float(outScale);
+    J.qOffC = float(isFloat ? 0.0 : 0.5 * outScale);
+    J.maxCode = isFloat ? 0 : (1 << J.bits) - 1;
+    for (int i = 0; i < 3; ++i) {
+        J.in[i] = t.in[i].data;
+        J.inPitch[i] = t.in[i].stride;
+        J.out[i] = t.out[i].data;
+        J.outPitch[i] = t.out[i].stride;
+    }
+    J.writeLuma = t.out[0].data != nullptr;
+
+    J.algo = p.algo;
+    J.kernel = int(p.k.kernel);
+    J.radial = p.k.radial;
+    J.guided = p.strength > 0.0;
+    J.sparse = J.guided && p.sparse;
+    J.ridge = p.ridge;
+    J.cedge = p.cedge;
+    J.bm = p.bm;
+    J.useMs = J.guided && p.ms > 0.0;
+    J.clampHull = p.arMargin >= 0.0;
+    J.trustOn = J.sparse;
+    const double trustThreshold = p.algo == 4 ? 0.25 * p.sigma : p.sigma;
+    J.trustThr = float(trustThreshold * trustThreshold);
+    J.dil = int(std::ceil(p.k.support * std::max(J.rw, J.rh))) + 8;
+    J.directOutput = F.directOutput(p);
+    J.needBackProject = F.needsBackProjection(p);
+    J.strength = p.algo == 4 ? 1.0f : float(p.strength);
+    J.strength4 = float(p.strength);
+    J.support = p.k.support;
+    J.sigma = float(p.sigma);
+    J.sratio = float(p.sratio);
+    J.sdb = float(p.sdb);
+    J.stretch = float(p.stretch);
+    J.invGsigma2 = 1.0f / float(p.gsigma * p.gsigma);
+    J.rescue = float(p.rescue);
+    J.msStrength = float(p.ms);
+    J.qgate = float(p.qgate);
+    J.margin = float(std::max(0.0, p.arMargin));
+    J.spOut = float(std::max(J.rw, J.rh));
+    J.bpGain = float(p.bp);
+    J.invWxC = float(std::min(1.0, double(J.W) / F.cw));
+    J.invWyC = float(std::min(1.0, double(J.H) / F.ch));
+    J.lut = F.dLut;
+    J.lutN = int(p.k.lut.size());
+    J.lutScale = p.k.lutScale;
+    J.lgfEps = p.reg * p.reg;
+
+    J.ax = T.ax; J.ay = T.ay; J.rad = T.rad;
+    J.lumaH = T.lumaH; J.lumaV = T.lumaV;
+    J.lcXb = T.lcXb; J.lcXe = T.lcXe; J.lcYb = T.lcYb; J.lcYe = T.lcYe;
+
+    // float input planes that are already packed are read in place
+    const bool packedY = isFloat && t.in[0].stride == (ptrdiff_t)F.sw * 4;
+    const bool packedU = isFloat && t.in[1].stride == (ptrdiff_t)F.cw * 4;
+    const bool packedV = isFloat && t.in[2].stride == (ptrdiff_t)F.cw * 4;
+    J.Yw = packedY ? nullptr : ws.Yw;
+    J.Uw = packedU ? nullptr : ws.Uw;
+    J.Vw = packedV ? nullptr : ws.Vw;
+    J.Y = packedY ? (const float *)t.in[0].data : ws.Yw;
+    J.U = packedU ? (const float *)t.in[1].data : ws.Uw;
+    J.V = packedV ? (const float *)t.in[2].data : ws.Vw;
+    J.jxx = ws.jxx; J.jxy = ws.jxy; J.jyy = ws.jyy;
+    J.lc = ws.lc; J.ms = ws.ms;
+    J.seed = ws.seed; J.mtmp = ws.mtmp; J.mask = ws.mask; J.cmask = ws.cmask;
+    J.oU = ws.oU; J.oV = ws.oV; J.lumaTmp = ws.lumaTmp;
+    J.counters = ws.counters;
+    // algo 6
+    J.aff = ws.aff; J.yc1 = ws.yc1; J.yc2 = ws.yc2;
+    J.detailTmp = ws.detailTmp; J.detailTmp2 = ws.detailTmp2;
+    J.ycH1 = T.ycH1; J.ycV1 = T.ycV1; J.ycH2 = T.ycH2; J.ycV2 = T.ycV2;
+    J.sax = T.sax; J.say = T.say; J.srad = T.srad;
+    J.nyqX = T.nyqX; J.nyqY = T.nyqY;
+    J.sinvWxC = float(std::min(1.0, double(F.sw) / F.cw));
+    J.sinvWyC = float(std::min(1.0, double(F.sh) / F.ch));
+    J.epsSig = (0.25 * p.sigma) * (0.25 * p.sigma);
+    if (p.algo == 6 && J.guided) {
+        const float *last = ((J.nyqX + J.nyqY) & 1) ? ws.detailTmp2 : ws.detailTmp;
+        J.detailSrc = last;
+        J.detail = J.sameSize ? const_cast<float *>(last) : ws.detail;
+    }
+    // algo 4
+    J.lgf = ws.lgf;
+    J.selW2 = ws.selW2; J.selW3 = ws.selW3; J.gU = ws.gU; J.gV = ws.gV;
+    J.roi = ws.roi;
+    J.lgfRoiOnly = (p.algo == 4 && isFloat) ? 1 : 0;
+    J.lsX = T.lsX; J.lsXf = T.lsXf; J.lsY = T.lsY; J.lsYf = T.lsYf;
+}
+
+// ---------------------------------------------------------------------------
+// stage scheduler
+// ---------------------------------------------------------------------------
+enum StageId : int {
+    S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_LC, S_DIL_H, S_DIL_V,
+    S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_RECON,
+    S_YC, S_AFFINE, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
+    S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
+    S_ROI, S_LGF_ROI, S_BLEND, S_STORE, S_N
+};
+
+int stageCount() { return S_N; }
+
+static inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+static int stageTiles(const FrameJob &J, int s) {
+    const bool resize = !J.sameSize;
+    if (s >= S_NYQ0 && s <= S_NYQ7) {
+        const int pass = s - S_NYQ0;
+        return (J.guided && J.algo == 6 && pass < J.nyqX + J.nyqY) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
+    }
+    switch (s) {
+    case S_CONVERT: return cdiv(J.sw, 32) * cdiv(J.sh, 8);
+    case S_LUMA_RADIAL: return (resize && J.writeLuma && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_LUMA_H: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
+    case S_LUMA_V: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_TENSOR: return J.guided ? cdiv(J.sw, 32) * cdiv(J.sh, 16) : 0;
+    case S_LC: return J.guided ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_DIL_H: return J.sparse ? cdiv(J.sw, 1024) * J.sh : 0;
+    case S_DIL_V: return J.sparse ? cdiv(J.sw, 32) * cdiv(J.sh, 128) : 0;
+    case S_MARK: return J.sparse ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_COUNT: return J.sparse ? cdiv(J.sw * J.sh, 1024) : 0;
+    case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_RECON: return cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_YC:
+    case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_DET_PLAIN: return (J.guided && J.algo == 6) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
+    case S_DET_RH: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
+    case S_DET_RV: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_DET_RR: return (J.guided && J.algo == 6 && resize && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_DET_TRANSFER: return (J.guided && J.algo == 6) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_ROI:
+    case S_BLEND: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_LGF_ROI: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_STORE: return J.directOutput ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
+    }
+    return 0;
+}
+
+void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan) {
+    const int n = int(jobs.size());
+    plan.prefix.assign(size_t(S_N) * (n + 1), 0);
+    plan.totals.assign(S_N, 0);
+    plan.maxDil = 0;
+    for (int s = 0; s < S_N; ++s) {
+        int acc = 0;
+        for (int f = 0; f < n; ++f) {
+            plan.prefix[size_t(s) * (n + 1) + f] = acc;
+            acc += stageTiles(jobs[f], s);
+        }
+        plan.prefix[size_t(s) * (n + 1) + n] = acc;
+        plan.totals[s] = acc;
+    }
+    for (const FrameJob &J : jobs)
+        if (J.sparse)
+            plan.maxDil = std::max(plan.maxDil, J.dil);
+}
+
+int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const FrameJob *dJobs,
+                 const int *dPrefix, cudaStream_t stream) {
+    const int n = int(jobs.size());
+    int launches = 0;
+    const dim3 b32x8(32, 8);
+    auto pre = [&](int s) { return dPrefix + size_t(s) * (n + 1); };
+    auto go = [&](int s, auto kernel, dim3 block, size_t smem = 0) {
+        if (plan.totals[s] == 0)
+            return;
+        kernel<<<plan.totals[s], block, smem, stream>>>(dJobs, pre(s), n);
+        ++launches;
+    };
+    go(S_CONVERT, k_convert, b32x8);
+    go(S_LUMA_RADIAL, k_luma_radial, b32x8);
+    go(S_LUMA_H, k_luma_h, b32x8);
+    go(S_LUMA_V, k_luma_v, b32x8);
+    go(S_TENSOR, k_tensor, dim3(32, 8));
+    go(S_LC, k_lc, b32x8);
+    go(S_DIL_H, k_dilate_h, dim3(256));
+    go(S_DIL_V, k_dilate_v, dim3(32), size_t(128 + 2 * plan.maxDil) * 32);
+    go(S_MARK, k_mark_chroma, b32x8);
+    go(S_COUNT, k_count, dim3(256));
+    go(S_GATE, k_gate, b32x8);
+    go(S_LGF_DENSE, k_lgf, b32x8);
+    go(S_RECON, k_recon, b32x8);
+    go(S_YC, k_yc_h, b32x8);
+    go(S_AFFINE, k_affine, b32x8);
+    go(S_DET_PLAIN, k_detail_plain, b32x8);
+    for (int pass = 0; pass < 8; ++pass) {
+        const int s = S_NYQ0 + pass;
+        if (plan.totals[s] == 0)
+            continue;
+        k_detail_nyq<<<plan.totals[s], b32x8, 0, stream>>>(dJobs, pre(s), n, pass);
+        ++launches;
+    }
+    go(S_DET_RH, k_detail_resize_h, b32x8);
+    go(S_DET_RV, k_detail_resize_v, b32x8);
+    go(S_DET_RR, k_detail_resize_radial, b32x8);
+    go(S_DET_TRANSFER, k_detail_transfer, b32x8);
+    go(S_ROI, k_roi, b32x8);
+    go(S_LGF_ROI, k_lgf, b32x8);
+    go(S_BLEND, k_blend, b32x8);
+    go(S_STORE, k_store_chroma, b32x8);
+    if (cudaPeekAtLastError() != cudaSuccess)
+        return -1;
+    return launches;
+}
+
+} // namespace lgcr_b200

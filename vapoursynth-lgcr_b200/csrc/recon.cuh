@@ -1,0 +1,257 @@
+// Device-side data layout and helpers of the Recon path.
+//
+// One FrameJob describes one frame: geometry, parameters, resident tables
+// and workspace planes, all in HBM. Every stage kernel takes an array of
+// FrameJobs plus a per-stage tile prefix table, so a single launch covers
+// one frame (the per-frame form) or a whole batch of uneven frames (the
+// batched form); a block finds its frame by binary search over the prefix.
+//
+// Arithmetic in these kernels follows the reference's scalar build operation
+// by operation (the library is compiled with -fmad=false, so no product is
+// fused into an add unless written as an fma whose result is provably the
+// same). The device helpers restate:
+//   bilinear / bilinearFast          src/lgcr.h:467-508
+//   principalTensorDirection         src/lgcr.h:516-538
+//   lutLookup                        src/lgcr.h:636-641
+//   floatToPlane quantizer           src/lgcr.h:997-1013
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lgcr_b200 {
+
+enum SampleKind : int { kU8 = 0, kU16 = 1, kF32 = 2 };
+
+struct AxisView {
+    int n, sup;
+    const int *start;
+    const float *w;          // n * sup
+    const uint8_t *am;       // n * sup
+    const float *wsum, *wabs;
+    const float *pos, *lpos;
+    const int *cbI0, *lbI0;
+    const float *cbF, *lbF;
+};
+
+struct RadialView {
+    int valid;
+    int supX, supY, phasesX;
+    const uint16_t *xPhase, *yPhase;
+    const float *weights;
+};
+
+struct WeightView {          // polyphase resampler table (luma resize etc.)
+    int n, sup;
+    const int *start;
+    const float *w;
+};
+
+// Counters written by the sparse stages (per frame).
+enum Counter : int {
+    kCntActiveOutput = 0,
+    kCntActiveChroma = 1,
+    kCntSeed = 2,
+    kCntMaskPixels = 3,
+    kCntRoi = 4,
+    kCntCount = 8
+};
+
+struct FrameJob {
+    // geometry
+    int sw, sh, cw, ch, W, H;
+    double rw, rh;
+    float rwF, rhF;
+    int sameSize;
+    // input / output
+    int inKind, outKind, bits;
+    double yScale, cOffset;            // planeToFloat (chroma offset)
+    float qScale, qOffC;               // floatToPlane scale / chroma offset
+    int maxCode;
+    const void *in[3];
+    long long inPitch[3];              // bytes
+    void *out[3];
+    long long outPitch[3];             // bytes
+    int writeLuma;                     // copy / resample luma into out[0]
+    // parameters
+    int algo, kernel, radial, sparse, ridge, cedge, bm;
+    int guided;                        // strength > 0
+    int useMs, clampHull, trustOn, dil;
+    int directOutput;                  // recon kernel quantizes and stores
+    int needBackProject;
+    float strength, sigma, sratio, sdb, stretch, invGsigma2, rescue;
+    float strength4;                   // algo 4 selector strength (lambda)
+    double support;                    // kernel support (luma radial resize)
+    float msStrength, qgate, margin, spOut, trustThr;
+    float bpGain;
+    float invWxC, invWyC;              // radial AA factors (chroma units)
+    float lutScale;
+    int lutN;
+    const float *lut;
+    // tables
+    AxisView ax, ay;
+    RadialView rad;
+    WeightView lumaH, lumaV;           // luma resize (separable)
+    const int *lcXb, *lcXe, *lcYb, *lcYe;
+    // workspace (packed planes, pitch == width)
+    const float *Y, *U, *V;            // source planes as float
+    float *Yw, *Uw, *Vw;               // conversion targets (== Y/U/V when converted)
+    float *jxx, *jxy, *jyy;            // sw x sh
+    float *lc, *ms;                    // cw x ch
+    uint8_t *seed, *mtmp, *mask;       // sw x sh
+    uint8_t *cmask;                    // cw x ch
+    float *oU, *oV;                    // W x H float output planes
+    float *lumaTmp;                    // W x sh luma resize intermediate
+    unsigned long long *counters;      // kCntCount
+    // algo 6 / algo 4 / bm workspaces
+    float *aff;                        // 9 chroma planes: aU aV g mnU mxU mnV mxV rng dgl
+    float *yc1, *yc2;                  // bilinear / bicubic degradation candidates
+    float *ycTmp;                      // cw x sh candidate intermediate (resize case)
+    float *detail;                     // sw x sh (or W x H) detail map
+    float *detailTmp, *detailTmp2;     // sw x sh scratch
+    WeightView ycH1, ycV1, ycH2, ycV2; // candidate degradation tables
+    WeightView detH, detV;             // detail resample to output (resize)
+    int nyqX, nyqY;                    // dyadic Nyquist passes per axis
+    AxisView sax, say;                 // source-grid plain axes (detail map)
+    RadialView srad;
+    const float *detailSrc;            // Nyquist-filtered detail on the source grid
+    double epsSig;                     // (0.25 sigma)^2
+    float sinvWxC, sinvWyC;            // radial AA factors of the source-grid axes
+    const int *lsX, *lsY;              // point-sampled luma axes (algo 4)
+    const float *lsXf, *lsYf;
+    int lgfRoiOnly;
+    float *lgf;                        // 6 chroma planes: aU bU confU aV bV confV
+    float *selW2, *selW3;              // W x H routing weights (float algo 4)
+    float *gU, *gV;                    // W x H guided values (float algo 4)
+    uint8_t *roi;                      // cw x ch
+    double lgfEps;
+    float *bmAcc;                      // 3 planes W x H (sumU, sumV, weight)
+    float *bmGuide;                    // W x H (resized guide when needed)
+    int *bmGroups;                     // per anchor: count + match coords
+    float *bmPatch;                    // per anchor filtered patches
+    int bmAnchorsX, bmAnchorsY;
+    const int *bmStartsX, *bmStartsY;
+    float bmSigma;
+};
+
+// ---------------------------------------------------------------------------
+// scalar helpers with the reference's std:: semantics
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+template <class T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+template <class T> __device__ __forceinline__ T sclamp(T v, T lo, T hi) {
+    return (v < lo) ? lo : (hi < v) ? hi : v;
+}
+__device__ __forceinline__ int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ float ldf(const float *p) { return __ldg(p); }
+
+// Block -> frame by binary search over the stage prefix table.
+__device__ __forceinline__ int findFrame(const int *tileStart, int njobs, int block) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(tileStart + mid) <= block) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// lgcr.h:467-475: bilinear sample with clamped fetches at a (double) position
+// that is always a float value here; the fraction is exact in float.
+__device__ __forceinline__ float bilinearAt(const float *p, int w, int h, float xf, float yf) {
+    const float flx = floorf(xf), fly = floorf(yf);
+    const int x0 = (int)flx, y0 = (int)fly;
+    const float fx = xf - flx;
+    const float fy = yf - fly;
+    const int xa = iclamp(x0, 0, w - 1), xb = iclamp(x0 + 1, 0, w - 1);
+    const int ya = iclamp(y0, 0, h - 1), yb = iclamp(y0 + 1, 0, h - 1);
+    const float a = ldf(p + (size_t)ya * w + xa), b = ldf(p + (size_t)ya * w + xb);
+    const float c = ldf(p + (size_t)yb * w + xa), d = ldf(p + (size_t)yb * w + xb);
+    return a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+}
+
+// lgcr.h:494-508: 4 direct loads with pre-clamped axis indices. Planes are
+// packed, so reads index the flat array exactly as the reference does.
+__device__ __forceinline__ float bilinearFast(const float *p, int w, int h, int x0, float fx,
+                                              int y0, float fy) {
+    if (w == 1) {
+        const float a = ldf(p + (size_t)y0 * w);
+        if (h == 1)
+            return a;
+        const float c = ldf(p + (size_t)(y0 + 1) * w);
+        return a + (c - a) * fy;
+    }
+    const float *r0 = p + (size_t)y0 * w + x0;
+    if (h == 1)
+        return ldf(r0) + (ldf(r0 + 1) - ldf(r0)) * fx;
+    const float *r1 = r0 + w;
+    const float a = ldf(r0), b = ldf(r0 + 1), c = ldf(r1), d = ldf(r1 + 1);
+    return a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+}
+
+struct TensorDir { float coherence, nx, ny; };
+
+// lgcr.h:516-538
+__device__ __forceinline__ TensorDir principalDirection(float jxx, float jxy, float jyy) {
+    TensorDir d{0.0f, 1.0f, 0.0f};
+    const float difference = jxx - jyy;
+    const float sum = jxx + jyy;
+    const float cross = 2.0f * jxy;
+    const float disc = sqrtf(difference * difference + cross * cross);
+    d.coherence = disc / (sum + 1e-12f);
+    if (disc <= 1e-20f)
+        return d;
+    float vx, vy;
+    if (difference >= 0.0f) {
+        vx = disc + difference;
+        vy = cross;
+    } else {
+        vx = cross;
+        vy = disc - difference;
+    }
+    const float inv = 1.0f / sqrtf(vx * vx + vy * vy);
+    d.nx = vx * inv;
+    d.ny = vy * inv;
+    return d;
+}
+
+// lgcr.h:636-641
+__device__ __forceinline__ float lutLookupDev(const float *lut, int n, float idx) {
+    int i0 = (int)idx;
+    i0 = iclamp(i0, 0, n - 2);
+    const float fr = smin(idx - (float)i0, 1.0f);
+    const float a = ldf(lut + i0);
+    return a + (ldf(lut + i0 + 1) - a) * fr;
+}
+
+// lgcr.h:1008: int(s*scale + off + 0.5f), clamped.
+__device__ __forceinline__ int quantize(float s, float scale, float off, int maxCode) {
+    const float t = s * scale + off + 0.5f;
+    const int v = __float2int_rz(t);
+    return v < 0 ? 0 : (v > maxCode ? maxCode : v);
+}
+
+// Store one chroma output sample in the output plane's type.
+__device__ __forceinline__ void storeChroma(const FrameJob &J, int plane, int x, int y, float v) {
+    char *row = static_cast<char *>(J.out[plane]) + (long long)y * J.outPitch[plane];
+    if (J.outKind == kF32) {
+        reinterpret_cast<float *>(row)[x] = v + 0.0f;   // s*1.0+0.0 in the reference
+    } else {
+        const int q = quantize(v, J.qScale, J.qOffC, J.maxCode);
+        if (J.outKind == kU8) reinterpret_cast<uint8_t *>(row)[x] = (uint8_t)q;
+        else reinterpret_cast<uint16_t *>(row)[x] = (uint16_t)q;
+    }
+}
+
+__device__ __forceinline__ void storeLuma(const FrameJob &J, int x, int y, float v) {
+    char *row = static_cast<char *>(J.out[0]) + (long long)y * J.outPitch[0];
+    if (J.outKind == kF32) {
+        reinterpret_cast<float *>(row)[x] = v + 0.0f;
+    } else {
+        const int q = quantize(v, J.qScale, 0.0f, J.maxCode);
+        if (J.outKind == kU8) reinterpret_cast<uint8_t *>(row)[x] = (uint8_t)q;
+        else reinterpret_cast<uint16_t *>(row)[x] = (uint16_t)q;
+    }
+}
+
+} // namespace lgcr_b200

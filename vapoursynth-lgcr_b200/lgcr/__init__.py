@@ -1,0 +1,288 @@
+"""B200-native LGCR Recon: Python mirror of the reference's `lgcr.Recon`.
+
+The reference registers `Recon` with VapourSynth as
+    clip:vnode; width,height,taps,algo,ridge,cedge,sparse,bm:int:opt;
+    kernel,loc:data:opt; b,c,strength,sigma,sratio,sdb,stretch,gsigma,rescue,
+    ar,reg,bp,ms,qgate:float:opt                      (src/plugin.cpp:1166-1171)
+This module exposes the same arguments and error messages over the C ABI in
+include/lgcr_b200.h (lgcr_recon_create / lgcr_recon_frame); frames are
+numpy planes (host memory) or CUDA torch tensors (device memory).
+
+The compute path is the CUDA library liblgcr_b200.so built in-tree; there is
+no CPU fallback: without the library or a GPU, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "liblgcr_b200.so")
+UNSET_INT = -(2 ** 31)
+
+LGCR_OK = 0
+LGCR_E_INVALID = 1
+LGCR_MEM_HOST = 0
+LGCR_MEM_DEVICE = 1
+
+INT_ARGS = ("width", "height", "taps", "algo", "ridge", "cedge", "sparse", "bm")
+FLOAT_ARGS = ("b", "c", "strength", "sigma", "sratio", "sdb", "stretch", "gsigma",
+              "rescue", "ar", "reg", "bp", "ms", "qgate")
+STR_ARGS = ("kernel", "loc")
+
+
+class Error(Exception):
+    """Raised where VapourSynth would raise vs.Error for Recon."""
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int),
+        ("kernel", ctypes.c_char_p), ("taps", ctypes.c_int), ("algo", ctypes.c_int),
+        ("b", ctypes.c_double), ("c", ctypes.c_double),
+        ("strength", ctypes.c_double), ("sigma", ctypes.c_double),
+        ("sratio", ctypes.c_double), ("sdb", ctypes.c_double),
+        ("stretch", ctypes.c_double), ("gsigma", ctypes.c_double),
+        ("rescue", ctypes.c_double),
+        ("ridge", ctypes.c_int), ("cedge", ctypes.c_int),
+        ("ar", ctypes.c_double), ("reg", ctypes.c_double),
+        ("loc", ctypes.c_char_p), ("sparse", ctypes.c_int),
+        ("bp", ctypes.c_double), ("ms", ctypes.c_double), ("qgate", ctypes.c_double),
+        ("bm", ctypes.c_int),
+    ]
+
+
+class Format(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "color_family", "sample_type", "bits_per_sample", "subsampling_w",
+        "subsampling_h", "width", "height")]
+
+
+class Plane(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("stride", ctypes.c_ssize_t),
+                ("width", ctypes.c_int), ("height", ctypes.c_int)]
+
+
+class FrameStats(ctypes.Structure):
+    _fields_ = [("output_pixels", ctypes.c_uint64),
+                ("sparse_active_pixels", ctypes.c_uint64),
+                ("sparse_total_pixels", ctypes.c_uint64),
+                ("active_output_pixels", ctypes.c_uint64),
+                ("active_chroma_pixels", ctypes.c_uint64),
+                ("sparse_active_ratio", ctypes.c_double),
+                ("device_ms", ctypes.c_double)]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("filter", ctypes.c_void_p), ("inp", Plane * 3), ("out", Plane * 3),
+                ("chroma_location", ctypes.c_int)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device_budget_bytes", ctypes.c_size_t), ("max_batch", ctypes.c_int),
+                ("lanes", ctypes.c_int), ("queue_capacity", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("submit_ms", ctypes.c_double),
+                ("start_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
+                ("batch_size", ctypes.c_int)]
+
+
+# Every entry point declared in include/lgcr_b200.h.
+EXPORTS = (
+    "lgcr_params_init", "lgcr_recon_create", "lgcr_recon_destroy",
+    "lgcr_recon_output_format", "lgcr_recon_frame", "lgcr_last_error",
+    "lgcr_batch_create", "lgcr_batch_destroy", "lgcr_batch_run",
+    "lgcr_batch_launch_count", "lgcr_autotune",
+    "lgcr_server_create", "lgcr_server_submit", "lgcr_server_wait", "lgcr_server_destroy",
+)
+
+_lib = None
+
+
+def library():
+    """Load liblgcr_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise Error(f"liblgcr_b200.so is missing ({LIBPATH}); build it with "
+                    "python vapoursynth-lgcr_b200/build.py")
+    lib = ctypes.CDLL(LIBPATH)
+    lib.lgcr_params_init.argtypes = [ctypes.POINTER(Params)]
+    lib.lgcr_recon_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(Format),
+                                      ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                                      ctypes.c_size_t]
+    lib.lgcr_recon_create.restype = ctypes.c_int
+    lib.lgcr_recon_destroy.argtypes = [ctypes.c_void_p]
+    lib.lgcr_recon_output_format.argtypes = [ctypes.c_void_p, ctypes.POINTER(Format)]
+    lib.lgcr_recon_frame.argtypes = [ctypes.c_void_p, ctypes.POINTER(Plane),
+                                     ctypes.POINTER(Plane), ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.POINTER(FrameStats)]
+    lib.lgcr_recon_frame.restype = ctypes.c_int
+    lib.lgcr_last_error.restype = ctypes.c_char_p
+    if hasattr(lib, "lgcr_batch_create"):
+        lib.lgcr_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+        lib.lgcr_batch_destroy.argtypes = [ctypes.c_void_p]
+        lib.lgcr_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_int]
+        lib.lgcr_batch_launch_count.argtypes = [ctypes.c_void_p]
+        lib.lgcr_autotune.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_char_p, ctypes.c_size_t]
+    if hasattr(lib, "lgcr_server_create"):
+        lib.lgcr_server_create.argtypes = [ctypes.POINTER(ServerConfig),
+                                           ctypes.POINTER(ctypes.c_void_p)]
+        lib.lgcr_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Plane),
+                                           ctypes.POINTER(Plane), ctypes.c_int]
+        lib.lgcr_server_submit.restype = ctypes.c_int64
+        lib.lgcr_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                         ctypes.POINTER(RequestInfo)]
+        lib.lgcr_server_destroy.argtypes = [ctypes.c_void_p]
+    _lib = lib
+    return lib
+
+
+def make_params(**kwargs) -> Params:
+    p = Params()
+    for name in INT_ARGS:
+        setattr(p, name, UNSET_INT)
+    for name in FLOAT_ARGS:
+        setattr(p, name, math.nan)
+    for name in STR_ARGS:
+        setattr(p, name, None)
+    for key, value in kwargs.items():
+        if value is None:
+            continue
+        if key in INT_ARGS:
+            setattr(p, key, int(value))
+        elif key in FLOAT_ARGS:
+            setattr(p, key, float(value))
+        elif key in STR_ARGS:
+            setattr(p, key, value.encode() if isinstance(value, str) else value)
+        else:
+            raise Error(f"Recon: argument {key!r} is not supported")
+    return p
+
+
+def video_format(width, height, bits=8, ssw=1, ssh=1, is_float=None) -> Format:
+    """Format of a planar YUV clip (bits 32 = float)."""
+    if is_float is None:
+        is_float = bits == 32
+    return Format(3, 1 if is_float else 0, 32 if is_float else bits, ssw, ssh, width, height)
+
+
+def format_of(planes, bits=None) -> Format:
+    """Format of a (Y, U, V) numpy/torch plane tuple."""
+    y, u, _ = planes
+    h, w = y.shape
+    ch, cw = u.shape
+    dt = str(getattr(y, "dtype", ""))
+    is_float = "float32" in dt
+    if bits is None:
+        bits = 32 if is_float else (8 if "uint8" in dt else 16)
+    ssw = 0 if cw == w else 1
+    ssh = 0 if ch == h else 1
+    return video_format(w, h, bits, ssw, ssh, is_float)
+
+
+def _plane_desc(a) -> Plane:
+    p = Plane()
+    if a is None:
+        return p
+    if hasattr(a, "data_ptr"):           # torch tensor
+        p.data = a.data_ptr()
+        p.stride = a.stride(0) * a.element_size()
+    else:
+        p.data = a.ctypes.data
+        p.stride = a.strides[0]
+    p.height, p.width = a.shape
+    return p
+
+
+def planes_desc(arrays):
+    arr = (Plane * 3)()
+    for i, a in enumerate(arrays):
+        arr[i] = _plane_desc(a)
+    return arr
+
+
+class Recon:
+    """One Recon filter instance (lgcrCreate); call frame() per frame."""
+
+    def __init__(self, fmt: Format, **kwargs):
+        self.lib = library()
+        self.fmt = fmt
+        self.params = make_params(**kwargs)
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        status = self.lib.lgcr_recon_create(ctypes.byref(self.params), ctypes.byref(fmt),
+                                            ctypes.byref(handle), err, 512)
+        if status != LGCR_OK:
+            raise Error(err.value.decode())
+        self.handle = handle
+        out = Format()
+        self.lib.lgcr_recon_output_format(self.handle, ctypes.byref(out))
+        self.out_w, self.out_h = out.width, out.height
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lgcr_recon_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def dtype(self):
+        if self.fmt.sample_type == 1:
+            return np.float32
+        return np.uint8 if self.fmt.bits_per_sample == 8 else np.uint16
+
+    def frame(self, planes, chroma_location: int = -1, out=None, stats: bool = False,
+              stream=None, share_luma: bool = False):
+        """Reconstruct one frame.
+
+        numpy planes run through host memory (upload, run, download);
+        CUDA tensors run in device memory on `stream` (a torch stream or
+        raw handle) without waiting unless stats=True."""
+        device = hasattr(planes[0], "data_ptr")
+        if out is None:
+            if device:
+                import torch
+                tdt = {np.uint8: torch.uint8, np.uint16: torch.uint16,
+                       np.float32: torch.float32}[self.dtype]
+                out = [torch.empty((self.out_h, self.out_w), dtype=tdt, device=planes[0].device)
+                       for _ in range(3)]
+            else:
+                out = [np.empty((self.out_h, self.out_w), dtype=self.dtype) for _ in range(3)]
+            if share_luma:
+                out[0] = None
+        else:
+            out = list(out)
+        if not device:
+            planes = [np.ascontiguousarray(p) for p in planes]
+        st = FrameStats()
+        handle = None
+        if stream is not None:
+            handle = getattr(stream, "cuda_stream", stream)
+        status = self.lib.lgcr_recon_frame(
+            self.handle, planes_desc(planes), planes_desc(out), int(chroma_location),
+            LGCR_MEM_DEVICE if device else LGCR_MEM_HOST, handle,
+            ctypes.byref(st) if stats else None)
+        if status != LGCR_OK:
+            raise Error(self.lib.lgcr_last_error().decode())
+        if stats:
+            return out, st
+        return out
+
+
+def recon(planes, chroma_location: int = -1, bits=None, **kwargs):
+    """One-shot Recon of a (Y, U, V) frame; returns the output planes."""
+    return Recon(format_of(planes, bits), **kwargs).frame(planes, chroma_location)
