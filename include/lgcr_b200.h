@@ -177,6 +177,16 @@ int lgcr_batch_run(lgcr_batch *batch, const lgcr_batch_item *items, int count,
 /* Number of kernel launches the last lgcr_batch_run enqueued. */
 int lgcr_batch_launch_count(const lgcr_batch *batch);
 
+/* Stage profiling (the reference's per-stage PipelineMetrics timers,
+ * src/pipeline.h:315-388, as CUDA events): when on, every stage launch of
+ * later runs is bracketed by events (graph replay is bypassed). */
+int lgcr_batch_set_profiling(lgcr_batch *batch, int on);
+/* Accumulated device ms and launch counts per stage since the last reset;
+ * waits for the recorded work. Arrays have lgcr_stage_count() entries. */
+int lgcr_batch_stage_times(lgcr_batch *batch, double *ms, int *launches, int reset);
+int lgcr_stage_count(void);
+const char *lgcr_stage_name(int stage);
+
 /* Autotuner: time the candidate launch shapes of every stage on the
  * given items and keep the fastest per stage (process-wide). */
 int lgcr_autotune(const lgcr_batch_item *items, int count, void *stream,

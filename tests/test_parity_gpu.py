@@ -79,3 +79,76 @@ def test_config0_shape_parity():
     got, ref = run_pair(planes, fmt, algo=2, kernel="lanczos", taps=3, strength=0.8,
                         sigma=0.01)
     assert_parity(got, ref, False, "config0")
+
+
+@pytest.mark.parametrize("fmt_name", ["420P8", "420P10", "420PS", "422P10", "444PS", "444P8"])
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("algo", [4, 6])
+@pytest.mark.parametrize("sparse", [0, 1])
+def test_algo46_same_size(fmt_name, kernel, algo, sparse):
+    fmt = FORMATS[fmt_name]
+    planes = S.make_frame(64, 48, fmt, seed=17)
+    got, ref = run_pair(planes, fmt, algo=algo, sparse=sparse, strength=0.8, **KERNELS[kernel])
+    assert_parity(got, ref, fmt.is_float, f"algo{algo} {fmt_name}/{kernel}/sparse={sparse}")
+
+
+@pytest.mark.parametrize("fmt_name", ["420P10", "420PS", "444P8"])
+@pytest.mark.parametrize("kernel", ["bilinear", "lanczos3", "spline36", "jinc3"])
+@pytest.mark.parametrize("algo", [4, 6])
+def test_algo46_resize(fmt_name, kernel, algo):
+    fmt = FORMATS[fmt_name]
+    planes = S.make_frame(48, 32, fmt, seed=19)
+    got, ref = run_pair(planes, fmt, algo=algo, width=70, height=44, **KERNELS[kernel])
+    assert_parity(got, ref, fmt.is_float, f"resize algo{algo} {fmt_name}/{kernel}")
+
+
+@pytest.mark.parametrize("fmt_name", ["420P8", "420P16", "420PS", "444PS"])
+@pytest.mark.parametrize("algo", [2, 6])
+@pytest.mark.parametrize("bp", [0.0, 1.0])
+def test_bm_bp(fmt_name, algo, bp):
+    fmt = FORMATS[fmt_name]
+    planes = S.make_frame(72, 56, fmt, seed=23, extra_noise=True)
+    got, ref = run_pair(planes, fmt, algo=algo, bm=1, bp=bp, kernel="lanczos", taps=3)
+    assert_parity(got, ref, fmt.is_float, f"bm {fmt_name}/algo{algo}/bp={bp}")
+
+
+@pytest.mark.parametrize("fmt_name", ["420P8", "420PS"])
+def test_bp_only(fmt_name):
+    fmt = FORMATS[fmt_name]
+    planes = S.make_frame(64, 40, fmt, seed=29)
+    got, ref = run_pair(planes, fmt, algo=2, bp=0.5)
+    assert_parity(got, ref, fmt.is_float, f"bp {fmt_name}")
+
+
+def test_bm_resize():
+    fmt = S.YUV420PS
+    planes = S.make_frame(48, 32, fmt, seed=31, extra_noise=True)
+    got, ref = run_pair(planes, fmt, width=80, height=56, bm=1)
+    assert_parity(got, ref, True, "bm resize")
+
+
+@pytest.mark.parametrize("algo", [2, 6])
+def test_config1_shape_1080p(algo):
+    """1920x1080 YUV420P10, lanczos4, sparse, qgate 1 (batched config frame)."""
+    fmt = S.YUV420P10
+    planes = S.make_frame(1920, 1080, fmt, seed=1000 + algo)
+    got, ref = run_pair(planes, fmt, algo=algo, kernel="lanczos", taps=4, sparse=1, qgate=1.0)
+    assert_parity(got, ref, False, f"config1 algo{algo}")
+
+
+@pytest.mark.parametrize("fmt_name", ["420P16", "420PS"])
+def test_config2_shape_jinc_resize(fmt_name):
+    """960x540 4:2:0 -> 1920x1080 jinc3 algo 4, reg 0.005 (config 2 at half size)."""
+    fmt = FORMATS[fmt_name]
+    planes = S.make_frame(960, 540, fmt, seed=2000, antialias=True)
+    got, ref = run_pair(planes, fmt, algo=4, kernel="jinc", taps=3, reg=0.005,
+                        width=1920, height=1080)
+    assert_parity(got, ref, fmt.is_float, f"config2 {fmt_name}")
+
+
+def test_config3_shape_bm_bp():
+    """1920x1080 YUV420P8, algo 2, bm, bp 1.0 (config 3 frame)."""
+    fmt = S.YUV420P8
+    planes = S.make_frame(1920, 1080, fmt, seed=3000, extra_noise=True)
+    got, ref = run_pair(planes, fmt, algo=2, bm=1, bp=1.0)
+    assert_parity(got, ref, False, "config3")

@@ -1,0 +1,268 @@
+// Batched form: many frames (any mix of filters, sizes, subsamplings and
+// depths) per launch of each stage. The launch sequence of a batch layout is
+// captured once into a CUDA graph and replayed; per-frame descriptors and
+// stage prefix tables are refreshed by copy nodes that read pinned host
+// buffers, so new frames (new plane pointers) replay the same graph.
+#include "impl.h"
+#include "kernels.cuh"
+
+#include <cstring>
+#include <string>
+
+using namespace lgcr_b200;
+
+struct StageEvent {
+    int stage;
+    cudaEvent_t start, stop;
+};
+
+struct lgcr_batch {
+    std::vector<std::unique_ptr<Workspace>> slots;
+    int capacity = 0;
+    FrameJob *dJobs = nullptr, *hJobs = nullptr;
+    int *dPrefix = nullptr, *hPrefix = nullptr;
+    size_t prefixCapacity = 0;
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+    // graph cache (one layout)
+    cudaGraphExec_t exec = nullptr;
+    std::string signature;
+    int lastLaunches = 0;
+    // profiling
+    bool profiling = false;
+    std::vector<StageEvent> events;
+    std::vector<cudaEvent_t> eventPool;
+    std::vector<double> stageMs;
+    std::vector<int> stageLaunches;
+    ~lgcr_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (dJobs) cudaFree(dJobs);
+        if (hJobs) cudaFreeHost(hJobs);
+        if (dPrefix) cudaFree(dPrefix);
+        if (hPrefix) cudaFreeHost(hPrefix);
+        if (done) cudaEventDestroy(done);
+        for (auto &e : events) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
+        for (auto e : eventPool) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+
+cudaEvent_t poolEvent(lgcr_batch *b) {
+    if (!b->eventPool.empty()) {
+        cudaEvent_t e = b->eventPool.back();
+        b->eventPool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+int ensureCapacity(lgcr_batch *b, int count) {
+    if (count <= b->capacity && size_t(stageCount()) * (count + 1) <= b->prefixCapacity)
+        return LGCR_OK;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->signature.clear(); }
+    if (b->dJobs) cudaFree(b->dJobs);
+    if (b->hJobs) cudaFreeHost(b->hJobs);
+    if (b->dPrefix) cudaFree(b->dPrefix);
+    if (b->hPrefix) cudaFreeHost(b->hPrefix);
+    const int cap = std::max(count, 8);
+    b->prefixCapacity = size_t(stageCount()) * (cap + 1);
+    if (cudaMalloc(&b->dJobs, sizeof(FrameJob) * cap) != cudaSuccess ||
+        cudaHostAlloc((void **)&b->hJobs, sizeof(FrameJob) * cap, cudaHostAllocDefault) != cudaSuccess ||
+        cudaMalloc(&b->dPrefix, b->prefixCapacity * sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc((void **)&b->hPrefix, b->prefixCapacity * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+        setError("LGCR: batch descriptor allocation failed");
+        return LGCR_E_NOMEM;
+    }
+    b->capacity = cap;
+    return LGCR_OK;
+}
+
+// Launch sequence; with profiling, each launched stage is bracketed by events.
+int enqueue(lgcr_batch *b, const std::vector<FrameJob> &jobs, const StagePlan &plan,
+            cudaStream_t s, bool copies) {
+    const int n = int(jobs.size());
+    if (copies) {
+        if (cudaMemcpyAsync(b->dJobs, b->hJobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(b->dPrefix, b->hPrefix, plan.prefix.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return -1;
+    }
+    if (!b->profiling)
+        return launchStages(jobs, plan, b->dJobs, b->dPrefix, s);
+    // profiled: one stage at a time so each launch gets its own events
+    int launches = 0;
+    StagePlan single = plan;
+    for (int st = 0; st < stageCount(); ++st) {
+        if (plan.totals[st] == 0)
+            continue;
+        for (int o = 0; o < stageCount(); ++o)
+            single.totals[o] = (o == st) ? plan.totals[st] : 0;
+        StageEvent ev{st, poolEvent(b), poolEvent(b)};
+        cudaEventRecord(ev.start, s);
+        const int l = launchStages(jobs, single, b->dJobs, b->dPrefix, s);
+        cudaEventRecord(ev.stop, s);
+        if (l < 0)
+            return -1;
+        launches += l;
+        b->events.push_back(ev);
+    }
+    return launches;
+}
+
+} // namespace
+
+extern "C" {
+
+int lgcr_batch_create(lgcr_batch **out) {
+    if (!out)
+        return LGCR_E_ARGUMENT;
+    auto b = std::make_unique<lgcr_batch>();
+    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        return cudaFail(cudaGetLastError(), "lgcr_batch_create");
+    b->stageMs.assign(stageCount(), 0.0);
+    b->stageLaunches.assign(stageCount(), 0);
+    *out = b.release();
+    return LGCR_OK;
+}
+
+void lgcr_batch_destroy(lgcr_batch *b) {
+    if (!b)
+        return;
+    cudaDeviceSynchronize();
+    delete b;
+}
+
+int lgcr_batch_launch_count(const lgcr_batch *b) { return b ? b->lastLaunches : 0; }
+
+int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void *stream,
+                   int use_graph) {
+    if (!b || !items || count <= 0) {
+        setError("LGCR: empty batch");
+        return LGCR_E_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int status = ensureCapacity(b, count);
+    if (status != LGCR_OK)
+        return status;
+    // the pinned descriptors are rewritten: the previous run must have read them
+    if (b->pending)
+        cudaEventSynchronize(b->done);
+    if ((int)b->slots.size() < count)
+        b->slots.resize(count);
+    std::vector<FrameJob> jobs(count);
+    std::string sig = std::to_string(count);
+    for (int i = 0; i < count; ++i) {
+        const lgcr_batch_item &it = items[i];
+        if (!it.filter) {
+            setError("LGCR: batch item without filter");
+            return LGCR_E_ARGUMENT;
+        }
+        Filter *F = it.filter->filter;
+        FrameTask t;
+        t.filter = F;
+        t.p = F->sited(it.chroma_location);
+        t.tables = F->tablesFor(t.p.shiftX, t.p.shiftY);
+        if (!t.tables) {
+            setError("LGCR: failed to upload geometry tables");
+            return LGCR_E_NOMEM;
+        }
+        if (!b->slots[i] || b->slots[i]->owner != F) {
+            b->slots[i] = F->makeWorkspace(false);
+            if (!b->slots[i]) {
+                setError("LGCR: device workspace allocation failed");
+                return LGCR_E_NOMEM;
+            }
+            b->signature.clear();
+        }
+        t.ws = b->slots[i].get();
+        for (int p = 0; p < 3; ++p) {
+            t.in[p] = it.in[p];
+            t.out[p] = it.out[p];
+        }
+        buildJob(t, jobs[i]);
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "|%p,%g,%g,%d,%d", (void *)F, t.p.shiftX, t.p.shiftY,
+                      t.out[0].data != nullptr, jobs[i].inKind);
+        sig += buf;
+    }
+    StagePlan plan;
+    planStages(jobs, plan);
+    std::memcpy(b->hJobs, jobs.data(), sizeof(FrameJob) * count);
+    std::memcpy(b->hPrefix, plan.prefix.data(), plan.prefix.size() * sizeof(int));
+    int launches = -1;
+    if (use_graph && !b->profiling) {
+        if (!b->exec || b->signature != sig) {
+            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+            cudaGraph_t graph = nullptr;
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                return cudaFail(cudaGetLastError(), "graph capture");
+            launches = enqueue(b, jobs, plan, s, true);
+            const cudaError_t e = cudaStreamEndCapture(s, &graph);
+            if (e != cudaSuccess || launches < 0)
+                return cudaFail(e != cudaSuccess ? e : cudaGetLastError(), "graph capture");
+            const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess)
+                return cudaFail(ie, "graph instantiate");
+            b->signature = sig;
+            b->lastLaunches = launches;
+        }
+        const cudaError_t e = cudaGraphLaunch(b->exec, s);
+        if (e != cudaSuccess)
+            return cudaFail(e, "graph launch");
+        launches = b->lastLaunches;
+    } else {
+        launches = enqueue(b, jobs, plan, s, true);
+        if (launches < 0)
+            return cudaFail(cudaGetLastError(), "lgcr_batch_run");
+        b->lastLaunches = launches;
+    }
+    cudaEventRecord(b->done, s);
+    b->pending = true;
+    return LGCR_OK;
+}
+
+// Stage profiling: bracket every stage launch of subsequent runs with CUDA
+// events (graphs are bypassed while on).
+int lgcr_batch_set_profiling(lgcr_batch *b, int on) {
+    if (!b)
+        return LGCR_E_ARGUMENT;
+    b->profiling = on != 0;
+    return LGCR_OK;
+}
+
+// Accumulated device milliseconds and launch counts per stage since the
+// last reset; waits for the recorded work. `ms`/`launches` have
+// lgcr_stage_count() entries (either may be NULL).
+int lgcr_batch_stage_times(lgcr_batch *b, double *ms, int *launches, int reset) {
+    if (!b)
+        return LGCR_E_ARGUMENT;
+    for (auto &e : b->events) {
+        cudaEventSynchronize(e.stop);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e.start, e.stop);
+        b->stageMs[e.stage] += t;
+        b->stageLaunches[e.stage] += 1;
+        b->eventPool.push_back(e.start);
+        b->eventPool.push_back(e.stop);
+    }
+    b->events.clear();
+    for (int i = 0; i < stageCount(); ++i) {
+        if (ms) ms[i] = b->stageMs[i];
+        if (launches) launches[i] = b->stageLaunches[i];
+    }
+    if (reset) {
+        std::fill(b->stageMs.begin(), b->stageMs.end(), 0.0);
+        std::fill(b->stageLaunches.begin(), b->stageLaunches.end(), 0);
+    }
+    return LGCR_OK;
+}
+
+int lgcr_stage_count(void) { return stageCount(); }
+
+const char *lgcr_stage_name(int stage) { return stageName(stage); }
+
+} // extern "C"

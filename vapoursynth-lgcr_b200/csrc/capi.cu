@@ -11,10 +11,6 @@ namespace lgcr_b200 {
 const char *lastError();
 }
 
-struct lgcr_recon {
-    Filter *filter;
-};
-
 namespace {
 
 int *zeroPrefix() {

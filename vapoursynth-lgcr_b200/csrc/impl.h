@@ -154,7 +154,13 @@ void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan);
 int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan,
                  const FrameJob *dJobs, const int *dPrefix, cudaStream_t stream);
 
+const char *stageName(int stage);
 const char *setError(const std::string &msg);
 int cudaFail(cudaError_t e, const char *where);
 
 } // namespace lgcr_b200
+
+// Handle type of the C ABI.
+struct lgcr_recon {
+    lgcr_b200::Filter *filter;
+};

@@ -326,6 +326,21 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         olsX = pk.add(bx.i0); olsXf = pk.add(bx.f);
         olsY = pk.add(by.i0); olsYf = pk.add(by.f);
     }
+    // bm: 8-px anchor grid plus the last full patch (blockStarts, bm.cpp:214-224)
+    auto blockStarts = [](int extent) {
+        std::vector<int> starts;
+        if (extent < 8)
+            return starts;
+        const int last = extent - 8;
+        for (int pos = 0; pos <= last; pos += 8)
+            starts.push_back(pos);
+        if (starts.empty() || starts.back() != last)
+            starts.push_back(last);
+        return starts;
+    };
+    const std::vector<int> bmX = p.bm ? blockStarts(p.outW) : std::vector<int>{};
+    const std::vector<int> bmY = p.bm ? blockStarts(p.outH) : std::vector<int>{};
+    const size_t obmX = pk.add(bmX), obmY = pk.add(bmY);
     std::vector<int> xb, xe, yb, ye;
     lcExtents(sw, cw, rw, shiftX, xb, xe);
     lcExtents(sh, ch, rh, shiftY, yb, ye);
@@ -370,6 +385,12 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         t->lsY = (const int *)t->arena.at(olsY);
         t->lsYf = (const float *)t->arena.at(olsYf);
     }
+    if (p.bm && !bmX.empty() && !bmY.empty()) {
+        t->bmStartsX = (const int *)t->arena.at(obmX);
+        t->bmStartsY = (const int *)t->arena.at(obmY);
+        t->bmAnchorsX = int(bmX.size());
+        t->bmAnchorsY = int(bmY.size());
+    }
     t->lcXb = (const int *)t->arena.at(oxb);
     t->lcXe = (const int *)t->arena.at(oxe);
     t->lcYb = (const int *)t->arena.at(oyb);
@@ -409,6 +430,8 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     const bool sel = algo4 && isFloat();
     Slot sW2 = take(O * 4, sel), sW3 = take(O * 4, sel), sGU = take(O * 4, sel), sGV = take(O * 4, sel);
     Slot sRoi = take(C, sel);
+    const size_t anchors = p.bm ? size_t((p.outW + 15) / 8) * ((p.outH + 15) / 8) : 0;
+    Slot sBmG = take(anchors * 9 * sizeof(int), p.bm), sBmP = take(anchors * 520 * 4, p.bm);
     Slot sIn[3], sOut[3];
     for (int i = 0; i < 3; ++i) {
         const size_t n = i == 0 ? L : C;
@@ -432,6 +455,8 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     ws->lgf = F(sLgf);
     ws->selW2 = F(sW2); ws->selW3 = F(sW3); ws->gU = F(sGU); ws->gV = F(sGV);
     ws->roi = B(sRoi);
+    ws->bmGroups = sBmG.on ? (int *)ar.at(sBmG.off) : nullptr;
+    ws->bmPatch = F(sBmP);
     for (int i = 0; i < 3; ++i) {
         const int w = i == 0 ? sw : cw;
         ws->stageIn[i] = sIn[i].on ? ar.at(sIn[i].off) : nullptr;
@@ -592,6 +617,13 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.roi = ws.roi;
     J.lgfRoiOnly = (p.algo == 4 && isFloat) ? 1 : 0;
     J.lsX = T.lsX; J.lsXf = T.lsXf; J.lsY = T.lsY; J.lsYf = T.lsYf;
+    // bm
+    J.bmGroups = ws.bmGroups; J.bmPatch = ws.bmPatch;
+    J.bmStartsX = T.bmStartsX; J.bmStartsY = T.bmStartsY;
+    J.bmAnchorsX = T.bmAnchorsX; J.bmAnchorsY = T.bmAnchorsY;
+    J.bmSigma = float(p.sigma);
+    if (!T.bmStartsX)
+        J.bm = 0;                                 // frame smaller than one patch
 }
 
 // ---------------------------------------------------------------------------
@@ -602,10 +634,27 @@ enum StageId : int {
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_RECON,
     S_YC, S_AFFINE, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
-    S_ROI, S_LGF_ROI, S_BLEND, S_STORE, S_N
+    S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
 
 int stageCount() { return S_N; }
+
+// Stage names; the ones with a reference counterpart use the reference's
+// stage vocabulary (stageName, src/pipeline.h:222-245).
+const char *stageName(int s) {
+    static const char *names[S_N] = {
+        "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
+        "buildGuideMaps_tensor", "buildGuideMaps_lc", "buildTrustMask_h", "buildTrustMask_v",
+        "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
+        "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_plain",
+        "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
+        "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
+        "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
+        "selector_roi", "buildLGF_roi", "selectorBlend", "collaborative_chroma_group",
+        "collaborative_chroma", "backProject", "output_conversion",
+    };
+    return (s >= 0 && s < S_N) ? names[s] : "unknown";
+}
 
 static inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 
@@ -638,6 +687,9 @@ static int stageTiles(const FrameJob &J, int s) {
     case S_DET_TRANSFER: return (J.guided && J.algo == 6) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_ROI:
     case S_BLEND: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_BM_GROUP: return J.bm ? cdiv(J.bmAnchorsX * J.bmAnchorsY, 8) : 0;
+    case S_BM_AGG: return J.bm ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_BP: return J.needBackProject ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_ROI: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_STORE: return J.directOutput ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
     }
@@ -705,6 +757,9 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_ROI, k_roi, b32x8);
     go(S_LGF_ROI, k_lgf, b32x8);
     go(S_BLEND, k_blend, b32x8);
+    go(S_BM_GROUP, k_bm_group, dim3(256));
+    go(S_BM_AGG, k_bm_aggregate, b32x8);
+    go(S_BP, k_backproject, b32x8);
     go(S_STORE, k_store_chroma, b32x8);
     if (cudaPeekAtLastError() != cudaSuccess)
         return -1;
