@@ -84,7 +84,7 @@ class Clocks:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -144,9 +144,21 @@ def cpu_threads():
     return max(1, min(n, 32))
 
 
-def run_cpu(frames, specs, steps, warmup, threads, per_step):
-    """Each step: `per_step` frames (round-robin over the workload) across
-    `threads` workers, one frame per worker at a time (fmParallel-like)."""
+def interleaved(specs):
+    """Workload order alternating 1080p and 4K frames, so any prefix samples
+    both sizes and both algorithms in proportion."""
+    small = [s["index"] for s in specs if s["width"] == 1920]
+    large = [s["index"] for s in specs if s["width"] != 1920]
+    order = []
+    for a, b in zip(small, large):
+        order += [a, b]
+    return order
+
+
+def run_cpu(frames, specs, steps, warmup, threads, per_step, min_seconds=0.0):
+    """Each step: `per_step` frames (round-robin over the interleaved
+    workload) across `threads` workers, one frame per worker at a time
+    (fmParallel-like). Steps repeat until `min_seconds` of timed work."""
     from oracle import oracle as O
     filters = {}
     for spec in specs:
@@ -157,8 +169,10 @@ def run_cpu(frames, specs, steps, warmup, threads, per_step):
                             for _ in range(threads)]
     times, pixels = [], []
     cursor = 0
-    for step in range(warmup + steps):
-        order = [(cursor + k) % len(specs) for k in range(per_step)]
+    sequence = interleaved(specs)
+    step = 0
+    while step < warmup + steps or sum(times) < min_seconds:
+        order = [sequence[(cursor + k) % len(sequence)] for k in range(per_step)]
         cursor += per_step
         lock = threading.Lock()
         queue = list(order)
@@ -183,6 +197,7 @@ def run_cpu(frames, specs, steps, warmup, threads, per_step):
         if step >= warmup:
             times.append(dt)
             pixels.append(sum(specs[i]["width"] * specs[i]["height"] for i in order))
+        step += 1
     total_s = sum(times)
     return sum(pixels) / total_s / 1e6, total_s, times
 
@@ -440,11 +455,13 @@ def our_arm(args):
     }
     if rank == 0 and cpu_frames is not None:
         threads = cpu_threads()
-        value_cpu, total_s, _ = run_cpu(cpu_frames, specs, 1, 0, threads, threads)
+        value_cpu, total_s, times = run_cpu(cpu_frames, specs, 1, 0, threads, threads,
+                                            min_seconds=10.0)
         result["cpu_baseline"] = {
             "value": round(value_cpu, 3), "unit": "Mpix/s", "cores": threads, "kind": "reference",
-            "sample": f"{threads} frames round-robin from the workload, one per thread, reference "
-                      f"AVX2 build (oracle/_ref), {total_s:.1f} s"}
+            "sample": f"{len(times)} rounds of {threads} frames (alternating 1080p/4K, algo 2/6, "
+                      f"one frame per thread) from the workload, reference AVX2 build "
+                      f"(oracle/_ref), {total_s:.1f} s"}
     lib.lgcr_batch_destroy(batch)
     if world > 1:
         torch.distributed.barrier()
@@ -457,7 +474,7 @@ def our_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

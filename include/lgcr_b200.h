@@ -153,6 +153,14 @@ int lgcr_recon_frame(lgcr_recon *filter, const lgcr_plane in[3],
 /* Text of the last error raised on the calling thread. */
 const char *lgcr_last_error(void);
 
+/* Diagnostics: the host-built chroma sampling axis the kernels index
+ * (buildChromaAxisUncached, src/kernels.cpp:337-404) for axis 0 (x) or 1
+ * (y) at siting `shift`. Arrays hold n entries (n*sup for w/am); any may be
+ * NULL. Returns the support in *sup. */
+int lgcr_debug_axis(const lgcr_recon *filter, int axis, double shift, int *start,
+                    float *w, uint8_t *am, float *pos, float *lpos, int *chroma_i0,
+                    float *chroma_f, int *luma_i0, float *luma_f, int *sup);
+
 /* ---------------------------------------------------------------------
  * Batched form: many frames (any mix of filters, sizes, subsamplings and
  * depths) in one launch per pipeline stage, captured as a CUDA graph and
@@ -221,6 +229,9 @@ int64_t lgcr_server_submit(lgcr_server *server, lgcr_recon *filter,
 /* Wait for a ticket (timeout_ms < 0 waits without limit). */
 int lgcr_server_wait(lgcr_server *server, int64_t ticket, int timeout_ms,
                      lgcr_request_info *info);
+/* Hold (on != 0) or release admission of queued requests (host-side
+ * control used to exercise bounded waits and admission). */
+int lgcr_server_pause(lgcr_server *server, int on);
 void lgcr_server_destroy(lgcr_server *server);
 
 #ifdef __cplusplus

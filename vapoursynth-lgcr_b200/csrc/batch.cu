@@ -266,3 +266,54 @@ int lgcr_stage_count(void) { return stageCount(); }
 const char *lgcr_stage_name(int stage) { return stageName(stage); }
 
 } // extern "C"
+
+// Autotuner: for every tunable per-pixel stage present in the given items,
+// time each candidate block (tile) shape with stage events and keep the
+// fastest; the choice applies process-wide to later plans.
+extern "C" int lgcr_autotune(const lgcr_batch_item *items, int count, void *stream,
+                             char *report, size_t reportlen) {
+    static const int cand[][2] = {{32, 8}, {16, 8}, {32, 4}, {64, 4}, {16, 16}, {128, 2}, {8, 8}};
+    lgcr_batch *b = nullptr;
+    int status = lgcr_batch_create(&b);
+    if (status != LGCR_OK)
+        return status;
+    lgcr_batch_set_profiling(b, 1);
+    std::string text;
+    std::vector<double> ms(stageCount());
+    for (int s = 0; s < stageCount() && status == LGCR_OK; ++s) {
+        if (!stageTunable(s))
+            continue;
+        int bestX, bestY;
+        stageShape(s, bestX, bestY);
+        double best = 1e300;
+        std::string line = std::string(stageName(s)) + ":";
+        for (const auto &c : cand) {
+            setStageShape(s, c[0], c[1]);
+            status = lgcr_batch_run(b, items, count, stream, 0);
+            if (status != LGCR_OK)
+                break;
+            lgcr_batch_stage_times(b, nullptr, nullptr, 1);
+            for (int rep = 0; rep < 2 && status == LGCR_OK; ++rep)
+                status = lgcr_batch_run(b, items, count, stream, 0);
+            lgcr_batch_stage_times(b, ms.data(), nullptr, 1);
+            if (ms[s] <= 0.0)
+                break;                         // stage not used by these items
+            char buf[64];
+            std::snprintf(buf, sizeof(buf), " %dx%d=%.3fms", c[0], c[1], ms[s] / 2);
+            line += buf;
+            if (ms[s] < best) { best = ms[s]; bestX = c[0]; bestY = c[1]; }
+        }
+        setStageShape(s, bestX, bestY);
+        if (best < 1e300) {
+            char buf[48];
+            std::snprintf(buf, sizeof(buf), " -> %dx%d\n", bestX, bestY);
+            text += line + buf;
+        }
+    }
+    lgcr_batch_destroy(b);
+    if (report && reportlen) {
+        std::strncpy(report, text.c_str(), reportlen - 1);
+        report[reportlen - 1] = '\0';
+    }
+    return status;
+}

@@ -200,4 +200,31 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
     return LGCR_OK;
 }
 
+int lgcr_debug_axis(const lgcr_recon *h, int axis, double shift, int *start, float *w,
+                    uint8_t *am, float *pos, float *lpos, int *ci0, float *cf, int *li0,
+                    float *lf, int *sup) {
+    if (!h || !sup)
+        return LGCR_E_ARGUMENT;
+    const Filter &F = *h->filter;
+    const int srcN = axis == 0 ? F.sw : F.sh;
+    const int dstN = axis == 0 ? F.p.outW : F.p.outH;
+    const double r = axis == 0 ? double(F.sw) / F.cw : double(F.sh) / F.ch;
+    const ChromaAxis a = buildChromaAxis(srcN, dstN, r, shift, F.p.k);
+    *sup = a.sup;
+    for (int i = 0; i < a.n; ++i) {
+        if (start) start[i] = a.start[i];
+        if (pos) pos[i] = a.pos[i];
+        if (lpos) lpos[i] = a.lpos[i];
+        if (ci0) ci0[i] = a.chromaBilin.i0[i];
+        if (cf) cf[i] = a.chromaBilin.f[i];
+        if (li0) li0[i] = a.lumaBilin.i0[i];
+        if (lf) lf[i] = a.lumaBilin.f[i];
+        for (int j = 0; j < a.sup; ++j) {
+            if (w) w[size_t(i) * a.sup + j] = a.w[size_t(i) * a.sup + j];
+            if (am) am[size_t(i) * a.sup + j] = a.am[size_t(i) * a.sup + j];
+        }
+    }
+    return LGCR_OK;
+}
+
 } // extern "C"

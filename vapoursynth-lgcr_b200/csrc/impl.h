@@ -155,6 +155,9 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan,
                  const FrameJob *dJobs, const int *dPrefix, cudaStream_t stream);
 
 const char *stageName(int stage);
+bool stageTunable(int stage);
+void stageShape(int stage, int &bx, int &by);
+void setStageShape(int stage, int bx, int by);
 const char *setError(const std::string &msg);
 int cudaFail(cudaError_t e, const char *where);
 

@@ -41,11 +41,12 @@ __global__ void k_bm_group(LGCR_STAGE_ARGS);
 __global__ void k_bm_aggregate(LGCR_STAGE_ARGS);
 __global__ void k_backproject(LGCR_STAGE_ARGS);
 
-// Tile helpers shared by the 32x8 per-pixel stages.
+// Tile helper of the per-pixel stages: the block shape (chosen by the
+// autotuner for the tunable stages) is the tile shape.
 __device__ __forceinline__ void tile32x8(int tile, int width, int &x, int &y) {
-    const int tilesX = (width + 31) / 32;
-    x = (tile % tilesX) * 32 + threadIdx.x;
-    y = (tile / tilesX) * 8 + threadIdx.y;
+    const int tilesX = (width + blockDim.x - 1) / blockDim.x;
+    x = (tile % tilesX) * blockDim.x + threadIdx.x;
+    y = (tile / tilesX) * blockDim.y + threadIdx.y;
 }
 
 } // namespace lgcr_b200

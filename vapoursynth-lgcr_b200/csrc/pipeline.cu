@@ -658,7 +658,53 @@ const char *stageName(int s) {
 
 static inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 
+// Launch shapes of the tunable per-pixel stages (process-wide; set by the
+// autotuner). Other stages use fixed shapes tied to their shared tiles.
+static std::mutex gShapeMu;
+static int gShapeX[S_N], gShapeY[S_N];
+static bool gShapeInit = false;
+
+static void initShapes() {
+    if (gShapeInit) return;
+    for (int i = 0; i < S_N; ++i) { gShapeX[i] = 32; gShapeY[i] = 8; }
+    gShapeInit = true;
+}
+
+bool stageTunable(int s) {
+    return s == S_RECON || s == S_AFFINE || s == S_DET_TRANSFER || s == S_DET_PLAIN ||
+           s == S_LGF_DENSE || s == S_YC || s == S_BM_AGG;
+}
+
+void stageShape(int s, int &bx, int &by) {
+    std::lock_guard<std::mutex> lock(gShapeMu);
+    initShapes();
+    bx = gShapeX[s]; by = gShapeY[s];
+}
+
+void setStageShape(int s, int bx, int by) {
+    std::lock_guard<std::mutex> lock(gShapeMu);
+    initShapes();
+    gShapeX[s] = bx; gShapeY[s] = by;
+}
+
+static int stageTilesShaped(const FrameJob &J, int s);
+
 static int stageTiles(const FrameJob &J, int s) {
+    if (stageTunable(s)) {
+        const int base = stageTilesShaped(J, s);
+        if (base == 0) return 0;
+        int bx, by;
+        stageShape(s, bx, by);
+        switch (s) {
+        case S_RECON: case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
+        case S_AFFINE: case S_LGF_DENSE: case S_YC: return cdiv(J.cw, bx) * cdiv(J.ch, by);
+        case S_DET_PLAIN: return cdiv(J.sw, bx) * cdiv(J.sh, by);
+        }
+    }
+    return stageTilesShaped(J, s);
+}
+
+static int stageTilesShaped(const FrameJob &J, int s) {
     const bool resize = !J.sameSize;
     if (s >= S_NYQ0 && s <= S_NYQ7) {
         const int pass = s - S_NYQ0;
@@ -724,6 +770,11 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     auto go = [&](int s, auto kernel, dim3 block, size_t smem = 0) {
         if (plan.totals[s] == 0)
             return;
+        if (stageTunable(s)) {
+            int bx, by;
+            stageShape(s, bx, by);
+            block = dim3(bx, by);
+        }
         kernel<<<plan.totals[s], block, smem, stream>>>(dJobs, pre(s), n);
         ++launches;
     };

@@ -125,23 +125,32 @@ def library():
                                      ctypes.c_void_p, ctypes.POINTER(FrameStats)]
     lib.lgcr_recon_frame.restype = ctypes.c_int
     lib.lgcr_last_error.restype = ctypes.c_char_p
-    if hasattr(lib, "lgcr_batch_create"):
-        lib.lgcr_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
-        lib.lgcr_batch_destroy.argtypes = [ctypes.c_void_p]
-        lib.lgcr_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int,
-                                       ctypes.c_void_p, ctypes.c_int]
-        lib.lgcr_batch_launch_count.argtypes = [ctypes.c_void_p]
-        lib.lgcr_autotune.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_void_p,
-                                      ctypes.c_char_p, ctypes.c_size_t]
-    if hasattr(lib, "lgcr_server_create"):
-        lib.lgcr_server_create.argtypes = [ctypes.POINTER(ServerConfig),
-                                           ctypes.POINTER(ctypes.c_void_p)]
-        lib.lgcr_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Plane),
-                                           ctypes.POINTER(Plane), ctypes.c_int]
-        lib.lgcr_server_submit.restype = ctypes.c_int64
-        lib.lgcr_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
-                                         ctypes.POINTER(RequestInfo)]
-        lib.lgcr_server_destroy.argtypes = [ctypes.c_void_p]
+    sigs = {
+        "lgcr_batch_create": ([ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+        "lgcr_batch_destroy": ([ctypes.c_void_p], None),
+        "lgcr_batch_run": ([ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int,
+                            ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+        "lgcr_batch_launch_count": ([ctypes.c_void_p], ctypes.c_int),
+        "lgcr_batch_set_profiling": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+        "lgcr_batch_stage_times": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+        "lgcr_stage_count": ([], ctypes.c_int),
+        "lgcr_stage_name": ([ctypes.c_int], ctypes.c_char_p),
+        "lgcr_autotune": ([ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_void_p,
+                           ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "lgcr_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)],
+                               ctypes.c_int),
+        "lgcr_server_submit": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Plane),
+                                ctypes.POINTER(Plane), ctypes.c_int], ctypes.c_int64),
+        "lgcr_server_wait": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                              ctypes.POINTER(RequestInfo)], ctypes.c_int),
+        "lgcr_server_destroy": ([ctypes.c_void_p], None),
+    }
+    for name, (args, res) in sigs.items():
+        if hasattr(lib, name):
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
     _lib = lib
     return lib
 
@@ -286,3 +295,53 @@ class Recon:
 def recon(planes, chroma_location: int = -1, bits=None, **kwargs):
     """One-shot Recon of a (Y, U, V) frame; returns the output planes."""
     return Recon(format_of(planes, bits), **kwargs).frame(planes, chroma_location)
+
+
+class Server:
+    """Continuous-batching request loop (lgcr_server_*): admission by a
+    device-memory budget, up to `max_batch` frames per device batch, `lanes`
+    batches in flight on separate streams."""
+
+    def __init__(self, budget_bytes=8 << 30, max_batch=8, lanes=2, queue_capacity=256):
+        self.lib = library()
+        self.lib.lgcr_server_pause.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        cfg = ServerConfig(int(budget_bytes), int(max_batch), int(lanes), int(queue_capacity))
+        handle = ctypes.c_void_p()
+        status = self.lib.lgcr_server_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if status != LGCR_OK:
+            raise Error(self.lib.lgcr_last_error().decode())
+        self.handle = handle
+        self._keep = {}
+
+    def submit(self, recon: "Recon", planes, out, chroma_location: int = -1) -> int:
+        """Queue one frame (host planes); returns a ticket, or a negative
+        status (-LGCR_E_BUSY when the queue is full or the frame exceeds the
+        budget)."""
+        ins, outs = planes_desc(planes), planes_desc(out)
+        ticket = self.lib.lgcr_server_submit(self.handle, recon.handle, ins, outs,
+                                             int(chroma_location))
+        if ticket >= 0:
+            self._keep[ticket] = (planes, out)
+        return ticket
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        info = RequestInfo()
+        status = self.lib.lgcr_server_wait(self.handle, int(ticket), int(timeout_ms),
+                                           ctypes.byref(info))
+        if status != 5:                 # LGCR_E_TIMEOUT keeps the request pending
+            self._keep.pop(ticket, None)
+        return status, info
+
+    def pause(self, on: bool):
+        self.lib.lgcr_server_pause(self.handle, 1 if on else 0)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lgcr_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
