@@ -37,6 +37,7 @@ PKG = os.path.join(ROOT, "vapoursynth-lgcr_b200")
 sys.path.insert(0, PKG)
 sys.path.insert(0, ROOT)
 
+from lgcr import replicas as R  # noqa: E402
 from lgcr import synthetic as S  # noqa: E402  (numpy only; no GPU)
 
 METRIC = "Recon 4:4:4 Mpix/s batched vs per-frame on 1 B200 at ≤1 LSB; p50/p99 ms"
@@ -51,7 +52,7 @@ def frame_specs(rank: int):
     for i in range(32):
         w, h = (1920, 1080) if i < 16 else (3840, 2160)
         specs.append(dict(index=i, width=w, height=h, algo=2 if i % 2 == 0 else 6,
-                          seed=1000 + 64 * rank + i))
+                          seed=R.frame_seed(1000, rank, i)))
     return specs
 
 
@@ -237,9 +238,7 @@ def reference_arm(args):
 # our arm
 # ---------------------------------------------------------------------------
 def our_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = R.rank_info()
     specs = frame_specs(rank)
     frames = generate(specs)                      # before CUDA init (spawn pool)
     cpu_frames = None
@@ -320,11 +319,7 @@ def our_arm(args):
     cnt_arr = (ctypes.c_int * nstages)()
     lib.lgcr_batch_stage_times(batch, ms_arr, cnt_arr, 1)
     stage_ms = {lib.lgcr_stage_name(i).decode(): ms_arr[i] for i in range(nstages) if cnt_arr[i]}
-    max_ms = elapsed_ms
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        max_ms = float(t.item())
+    max_ms = R.max_over_ranks(elapsed_ms, dev)
     value = out_pixels * world * args.steps / (max_ms / 1000.0) / 1e6
 
     # correctness spot check of the timed output (first 1080p frame) vs a
@@ -403,10 +398,7 @@ def our_arm(args):
         e2e_pass()
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = R.max_over_ranks(e2e_s, dev)
     e2e_value = out_pixels * world * args.steps / e2e_s / 1e6
     out_bytes_e2e = sum(2 * s["width"] * s["height"] * 2 for s in specs)   # U, V (luma shared)
 
