@@ -153,6 +153,23 @@ int lgcr_recon_frame(lgcr_recon *filter, const lgcr_plane in[3],
 /* Text of the last error raised on the calling thread. */
 const char *lgcr_last_error(void);
 
+/*
+ * lgcr_recon_frame_static: lgcr_recon_frame for device planes that
+ * allocates no device memory. No counterpart in the reference (which runs on
+ * the CPU); it exists for callers that cannot call cudaMalloc -- hosts that
+ * own all device memory through their own pool, or latency-critical paths
+ * where an allocation would synchronize the device.
+ * Scratch lives in one library-wide device array of 64 MiB (held on every
+ * GPU that loads the library until exit): frames needing more, and algo 4/6
+ * with strength > 0, bm or bp, are rejected with LGCR_E_ARGUMENT and a
+ * message. The first call on a device looks up the array's address and
+ * should come before any stream capture. All calls share the array: calls
+ * whose work overlaps on the GPU race and must be ordered by the caller.
+ * Work is enqueued on `stream` (a cudaStream_t); the call does not wait.
+ */
+int lgcr_recon_frame_static(lgcr_recon *filter, const lgcr_plane in[3],
+                            const lgcr_plane out[3], int chroma_location, void *stream);
+
 /* Diagnostics: the host-built chroma sampling axis the kernels index
  * (buildChromaAxisUncached, src/kernels.cpp:337-404) for axis 0 (x) or 1
  * (y) at siting `shift`. Arrays hold n entries (n*sup for w/am); any may be

@@ -1,0 +1,86 @@
+"""lgcr_recon_frame_static (the entry point that allocates no device memory,
+for callers that cannot call cudaMalloc) against lgcr_recon_frame on the
+same frames, two calls in a row, through the C ABI. Collected last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import assert_parity
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import lgcr
+from lgcr import synthetic as S
+
+
+def bind():
+    lib = lgcr.library()
+    fn = lib.lgcr_recon_frame_static
+    fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(lgcr.Plane), ctypes.POINTER(lgcr.Plane),
+                   ctypes.c_int, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return lib, fn
+
+
+def to_device(planes):
+    out = []
+    for p in planes:
+        if p.dtype == np.uint16:
+            out.append(torch.from_numpy(p.view(np.int16)).cuda().view(torch.uint16))
+        else:
+            out.append(torch.from_numpy(p).cuda())
+    return out
+
+
+def empty_like_out(rec, dev_planes):
+    return [torch.empty((rec.out_h, rec.out_w), dtype=dev_planes[0].dtype, device="cuda")
+            for _ in range(3)]
+
+
+@pytest.mark.parametrize("fmt,geom,kw", [
+    (S.YUV420P10, (640, 360), dict(algo=2, kernel="lanczos", taps=4)),
+    (S.YUV420PS, (320, 180), dict(algo=2, kernel="jinc", taps=3, width=480, height=270)),
+    (S.YUV422P10, (256, 144), dict(algo=6, strength=0.0, kernel="spline36")),
+])
+def test_static_matches_regular_twice(fmt, geom, kw):
+    lib, fn = bind()
+    w, h = geom
+    rec = lgcr.Recon(lgcr.video_format(w, h, fmt.bits, fmt.ssw, fmt.ssh), **kw)
+    stream = torch.cuda.current_stream().cuda_stream
+    for call, seed in enumerate((71, 72)):          # two calls in a row
+        planes = S.make_frame(w, h, fmt, seed=seed)
+        dev = to_device(planes)
+        ref = empty_like_out(rec, dev)
+        got = empty_like_out(rec, dev)
+        rec.frame(dev, -1, out=ref, stream=stream)
+        status = fn(rec.handle, lgcr.planes_desc(dev), lgcr.planes_desc(got), -1, stream)
+        assert status == 0, lib.lgcr_last_error().decode()
+        torch.cuda.synchronize()
+        host = lambda planes_: [p.cpu().numpy() if p.dtype != torch.uint16
+                                else p.view(torch.int16).cpu().numpy().view(np.uint16)
+                                for p in planes_]
+        assert_parity(host(got), host(ref), fmt.is_float, f"static call {call}")
+
+
+def test_static_rejects_oversize_and_unsupported():
+    lib, fn = bind()
+    big = lgcr.Recon(lgcr.video_format(3840, 2160, 10, 1, 1))
+    planes = [torch.zeros((2160, 3840), dtype=torch.uint16, device="cuda"),
+              torch.zeros((1080, 1920), dtype=torch.uint16, device="cuda"),
+              torch.zeros((1080, 1920), dtype=torch.uint16, device="cuda")]
+    outs = [torch.zeros((2160, 3840), dtype=torch.uint16, device="cuda") for _ in range(3)]
+    stream = torch.cuda.current_stream().cuda_stream
+    assert fn(big.handle, lgcr.planes_desc(planes), lgcr.planes_desc(outs), -1, stream) != 0
+    assert "scratch" in lib.lgcr_last_error().decode()
+    bm = lgcr.Recon(lgcr.video_format(64, 48, 8, 1, 1), bm=1)
+    p8 = [torch.zeros((48, 64), dtype=torch.uint8, device="cuda"),
+          torch.zeros((24, 32), dtype=torch.uint8, device="cuda"),
+          torch.zeros((24, 32), dtype=torch.uint8, device="cuda")]
+    o8 = [torch.zeros((48, 64), dtype=torch.uint8, device="cuda") for _ in range(3)]
+    assert fn(bm.handle, lgcr.planes_desc(p8), lgcr.planes_desc(o8), -1, stream) != 0
+    assert "bm" in lib.lgcr_last_error().decode()
