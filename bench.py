@@ -297,6 +297,14 @@ def our_arm(args):
         if world > 1:
             torch.distributed.barrier()
 
+    # autotune launch shapes / register budget on this workload (untimed)
+    tuned = ""
+    if not args.no_autotune:
+        rep = ctypes.create_string_buffer(4096)
+        if lib.lgcr_autotune(items, len(specs), ctypes.c_void_p(sh), rep, 4096) == 0:
+            tuned = rep.value.decode()
+        torch.cuda.synchronize(dev)
+
     # warm-up (also builds tables, workspaces, the graph)
     lib.lgcr_batch_set_profiling(batch, 1)
     for _ in range(max(args.warmup, 1)):
@@ -430,7 +438,8 @@ def our_arm(args):
                    "output_mpix_per_step": round(out_pixels / 1e6, 3),
                    "l2": "inputs larger than L2: ~250 MB in + 1 GB out per step",
                    "accumulation": "f32 with f64 accumulators (as the reference)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "autotune": [l for l in tuned.splitlines() if l]},
         "per_frame": {"value": round(out_pixels * args.steps / (per_frame_ms / 1000) / 1e6, 2),
                       "unit": "Mpix/s", "ms_per_step": round(per_frame_ms / args.steps, 3)},
         "graph_replay": {"value": round(out_pixels * args.steps / (graph_ms / 1000) / 1e6, 2),
@@ -470,6 +479,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

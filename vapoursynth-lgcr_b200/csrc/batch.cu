@@ -310,6 +310,33 @@ extern "C" int lgcr_autotune(const lgcr_batch_item *items, int count, void *stre
             text += line + buf;
         }
     }
+    // register budget of the persistent guided stage
+    if (status == LGCR_OK) {
+        int guidedStage = -1;
+        for (int s = 0; s < stageCount(); ++s)
+            if (std::string(stageName(s)) == "reconstructChroma")
+                guidedStage = s;
+        double best = 1e300;
+        int bestV = guidedVariant();
+        std::string line = "reconstructChroma:";
+        for (int v = 0; v < 2 && guidedStage >= 0 && status == LGCR_OK; ++v) {
+            setGuidedVariant(v);
+            status = lgcr_batch_run(b, items, count, stream, 0);
+            lgcr_batch_stage_times(b, nullptr, nullptr, 1);
+            for (int rep = 0; rep < 2 && status == LGCR_OK; ++rep)
+                status = lgcr_batch_run(b, items, count, stream, 0);
+            lgcr_batch_stage_times(b, ms.data(), nullptr, 1);
+            if (ms[guidedStage] <= 0.0)
+                break;
+            char buf[64];
+            std::snprintf(buf, sizeof(buf), " %d-blocks=%.3fms", v ? 3 : 2, ms[guidedStage] / 2);
+            line += buf;
+            if (ms[guidedStage] < best) { best = ms[guidedStage]; bestV = v; }
+        }
+        setGuidedVariant(bestV);
+        if (best < 1e300)
+            text += line + (bestV ? " -> 3 blocks/SM\n" : " -> 2 blocks/SM\n");
+    }
     lgcr_batch_destroy(b);
     if (report && reportlen) {
         std::strncpy(report, text.c_str(), reportlen - 1);

@@ -87,8 +87,11 @@ struct Workspace {
     uint8_t *seed = nullptr, *mtmp = nullptr, *mask = nullptr, *cmask = nullptr;
     float *oU = nullptr, *oV = nullptr, *lumaTmp = nullptr;
     unsigned long long *counters = nullptr;
+    double *uvd = nullptr;
+    float *hTab = nullptr;
+    uint32_t *actList = nullptr;
     float *aff = nullptr, *yc1 = nullptr, *yc2 = nullptr, *ycTmp = nullptr;
-    float *detail = nullptr, *detailTmp = nullptr, *detailTmp2 = nullptr;
+    float *detail = nullptr, *detailTmp = nullptr, *detailTmp2 = nullptr, *dTab = nullptr;
     float *lgf = nullptr, *selW2 = nullptr, *selW3 = nullptr, *gU = nullptr, *gV = nullptr;
     uint8_t *roi = nullptr;
     float *bmAcc = nullptr, *bmGuide = nullptr, *bmPatch = nullptr;
@@ -158,6 +161,8 @@ const char *stageName(int stage);
 bool stageTunable(int stage);
 void stageShape(int stage, int &bx, int &by);
 void setStageShape(int stage, int bx, int by);
+int guidedVariant();
+void setGuidedVariant(int variant);
 const char *setError(const std::string &msg);
 int cudaFail(cudaError_t e, const char *where);
 

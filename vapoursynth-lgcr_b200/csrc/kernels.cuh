@@ -17,7 +17,10 @@ __global__ void k_dilate_v(LGCR_STAGE_ARGS);
 __global__ void k_mark_chroma(LGCR_STAGE_ARGS);
 __global__ void k_count(LGCR_STAGE_ARGS);
 __global__ void k_gate(LGCR_STAGE_ARGS);
-__global__ void k_recon(LGCR_STAGE_ARGS);
+__global__ void k_hpass(LGCR_STAGE_ARGS);
+__global__ void k_plain(LGCR_STAGE_ARGS);
+__global__ void k_guided(LGCR_STAGE_ARGS);
+__global__ void k_guided3(LGCR_STAGE_ARGS);
 __global__ void k_luma_h(LGCR_STAGE_ARGS);
 __global__ void k_luma_v(LGCR_STAGE_ARGS);
 __global__ void k_luma_radial(LGCR_STAGE_ARGS);
@@ -25,6 +28,7 @@ __global__ void k_store_chroma(LGCR_STAGE_ARGS);
 // algo 6
 __global__ void k_yc_h(LGCR_STAGE_ARGS);
 __global__ void k_affine(LGCR_STAGE_ARGS);
+__global__ void k_detail_hpass(LGCR_STAGE_ARGS);
 __global__ void k_detail_plain(LGCR_STAGE_ARGS);
 __global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass);
 __global__ void k_detail_resize_h(LGCR_STAGE_ARGS);

@@ -132,6 +132,35 @@ k_affine(LGCR_STAGE_ARGS) {
     A[7 * C + o] = smax(mxU - mnU, mxV - mnV);
 }
 
+// Horizontal pass of the degraded-luma reconstruction (separable kernels):
+// per (source luma column, chroma row) the double sum over the active taps
+// rounded to float, and the row's extrema (plainChromaSeparable with one
+// plane, src/recon.cpp:1178-1271).
+__global__ void __launch_bounds__(256)
+k_detail_hpass(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int x, sy;
+    tile32x8(blockIdx.x - tileStart[f], J.sw, x, sy);
+    if (x >= J.sw || sy >= J.ch)
+        return;
+    const AxisView &ax = J.sax;
+    const int tx0 = __ldg(ax.start + x);
+    const double *wx = ax.wd + (size_t)x * ax.sup;
+    const uint8_t *amx = ax.am + (size_t)x * ax.sup;
+    const float *row = J.aff + 8 * (size_t)J.cw * J.ch + (size_t)sy * J.cw;
+    double h = 0.0;
+    float mn = 1e30f, mx = -1e30f;
+    for (int i = 0; i < ax.sup; ++i) {
+        if (__ldg(amx + i) == 0)
+            continue;
+        const float a = ldf(row + iclamp(tx0 + i, 0, J.cw - 1));
+        h = fma(__ldg(wx + i), (double)a, h);
+        mn = smin(mn, a); mx = smax(mx, a);
+    }
+    reinterpret_cast<float4 *>(J.dTab)[(size_t)sy * J.sw + x] = make_float4((float)h, mn, mx, 0.0f);
+}
+
 // detail = Y - plain(D(Y)) on the source luma grid.
 __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -140,6 +169,36 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     tile32x8(blockIdx.x - tileStart[f], J.sw, x, y);
     if (x >= J.sw || y >= J.sh)
         return;
+    const size_t o = (size_t)y * J.sw + x;
+    if (J.dTab) {
+        // vertical pass over the horizontal table
+        const AxisView &ax = J.sax, &ay = J.say;
+        const int ty0 = __ldg(ay.start + y);
+        const double *wy = ay.wd + (size_t)y * ay.sup;
+        const uint8_t *amy = ay.am + (size_t)y * ay.sup;
+        double v = 0.0;
+        float mn = 1e30f, mx = -1e30f;
+#pragma unroll 8
+        for (int j = 0; j < ay.sup; ++j) {
+            if (__ldg(amy + j) == 0)
+                continue;
+            const int sy = iclamp(ty0 + j, 0, J.ch - 1);
+            const float4 t = __ldg(reinterpret_cast<const float4 *>(J.dTab) + (size_t)sy * J.sw + x);
+            v = fma(__ldg(wy + j), (double)t.x, v);
+            mn = smin(mn, t.y); mx = smax(mx, t.z);
+        }
+        const double ws = (double)__ldg(ax.wsum + x) * (double)__ldg(ay.wsum + y);
+        const double wa = (double)__ldg(ax.wabs + x) * (double)__ldg(ay.wabs + y);
+        const float *dgl = J.aff + 8 * (size_t)J.cw * J.ch;
+        if (ws > 1e-6 && ws >= 0.05 * wa)
+            v /= ws;
+        else
+            v = bilinearAt(dgl, J.cw, J.ch, __ldg(ax.pos + x), __ldg(ay.pos + y));
+        if (J.clampHull)
+            v = sclamp(v, (double)(mn - J.margin), (double)(mx + J.margin));
+        J.detailTmp[o] = ldf(J.Y + o) - (float)v;
+        return;
+    }
     PlainCtx c = chromaPlainCtx(J);
     c.p0 = J.aff + 8 * (size_t)J.cw * J.ch;
     c.p1 = nullptr;
@@ -150,7 +209,6 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     c.invWyC = J.sinvWyC;
     float r, unused;
     plainAt(c, x, y, r, unused);
-    const size_t o = (size_t)y * J.sw + x;
     J.detailTmp[o] = ldf(J.Y + o) - r;
 }
 

@@ -47,10 +47,13 @@ __global__ void k_convert(const FrameJob *__restrict__ jobs, const int *__restri
         else reinterpret_cast<float *>(dst)[x] = reinterpret_cast<const float *>(src)[x];
     }
     if (x < J.cw && y < J.ch) {
-        if (J.cmask) J.cmask[(size_t)y * J.cw + x] = 0;
-        if (J.roi) J.roi[(size_t)y * J.cw + x] = 0;
-        if (J.Uw) J.Uw[(size_t)y * J.cw + x] = loadSample(J, 1, x, y);
-        if (J.Vw) J.Vw[(size_t)y * J.cw + x] = loadSample(J, 2, x, y);
+        const size_t o = (size_t)y * J.cw + x;
+        if (J.cmask) J.cmask[o] = 0;
+        if (J.roi) J.roi[o] = 0;
+        const float u = loadSample(J, 1, x, y), v = loadSample(J, 2, x, y);
+        if (J.Uw) J.Uw[o] = u;
+        if (J.Vw) J.Vw[o] = v;
+        if (J.uvd) reinterpret_cast<double2 *>(J.uvd)[o] = make_double2((double)u, (double)v);
     }
 }
 
@@ -273,8 +276,8 @@ __global__ void k_mark_chroma(const FrameJob *__restrict__ jobs, const int *__re
     const int oy = (tile / tilesX) * 8 + threadIdx.y;
     bool active = false;
     if (ox < J.W && oy < J.H) {
-        active = outputActive(J, ox, oy);
-        if (active) {
+        active = J.sparse ? outputActive(J, ox, oy) : true;
+        if (active && J.sparse) {
             const int cx0 = __ldg(J.ax.cbI0 + ox);
             const int cx1 = min(cx0 + 1, J.cw - 1);
             const int cy0 = __ldg(J.ay.cbI0 + oy);
@@ -286,9 +289,30 @@ __global__ void k_mark_chroma(const FrameJob *__restrict__ jobs, const int *__re
             m[(size_t)cy1 * J.cw + cx1] = 1;
         }
     }
+    // block-aggregated append to the frame's guided work list: one atomic
+    // per block (8 warps), warp offsets from a shared prefix
+    __shared__ unsigned warpCount[8];
+    __shared__ unsigned long long blockBase;
     const unsigned ballot = __ballot_sync(0xffffffffu, active);
-    if ((threadIdx.x & 31) == 0 && ballot)
-        atomicAdd(J.counters + kCntActiveOutput, (unsigned long long)__popc(ballot));
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0)
+        warpCount[warp] = __popc(ballot);
+    __syncthreads();
+    if (tid == 0) {
+        unsigned total = 0;
+        for (int w = 0; w < 8; ++w) {
+            const unsigned c = warpCount[w];
+            warpCount[w] = total;
+            total += c;
+        }
+        blockBase = total ? atomicAdd(J.counters + kCntActiveOutput, (unsigned long long)total) : 0ull;
+    }
+    __syncthreads();
+    if (active && J.listed) {
+        const unsigned rank = warpCount[warp] + __popc(ballot & ((1u << lane) - 1u));
+        J.actList[blockBase + rank] = ((uint32_t)oy << 16) | (uint32_t)ox;
+    }
 }
 
 // Population count of a u8 plane region: counts chroma mask / trust mask.
@@ -309,9 +333,17 @@ __global__ void k_count(const FrameJob *__restrict__ jobs, const int *__restrict
         c += __shfl_down_sync(0xffffffffu, c, o);
         m += __shfl_down_sync(0xffffffffu, m, o);
     }
+    __shared__ int sc[8], sm[8];
     if ((threadIdx.x & 31) == 0) {
-        if (c) atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)c);
-        if (m) atomicAdd(J.counters + kCntMaskPixels, (unsigned long long)m);
+        sc[threadIdx.x >> 5] = c;
+        sm[threadIdx.x >> 5] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tc = 0, tm = 0;
+        for (int w = 0; w < 8; ++w) { tc += sc[w]; tm += sm[w]; }
+        if (tc) atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)tc);
+        if (tm) atomicAdd(J.counters + kCntMaskPixels, (unsigned long long)tm);
     }
 }
 

@@ -1,10 +1,20 @@
-// Chroma reconstruction stage: one thread per output pixel.
-//   plain separable   plainChromaSeparable (scalar)   src/recon.cpp:1151-1461
-//   plain bilinear    plainChromaBilinear             src/recon.cpp:1031-1149
-//   plain radial      plainChromaImpl<radial>         src/recon.cpp:828-1029
-//   guided            reconstructChromaImpl (scalar)  src/recon.cpp:14-819
-//   luma resize       resampleH/V, resampleRadial     src/kernels.cpp:171-334
-//   output store      floatToPlane                    src/lgcr.h:997-1013
+// Chroma reconstruction stages.
+//   k_hpass   horizontal pass of the separable kernels: per (output column,
+//             chroma row) the plain horizontal sums of U, V and the window
+//             extrema of U, V, lc over the active taps (the reference's
+//             ring rows, plainChromaSeparable src/recon.cpp:1178-1271)
+//   k_plain   plain base per output pixel: vertical pass over the table
+//             (separable, src/recon.cpp:1281-1437), bilinear
+//             (src/recon.cpp:1031-1149) or radial (src/recon.cpp:828-1029);
+//             writes the final sample of pixels the guided pass skips
+//   k_guided  reconstructChromaImpl (scalar, src/recon.cpp:14-819) for the
+//             active pixels of every frame in the launch: a persistent grid
+//             walks the frames' compacted work lists (no divergence between
+//             plain and guided pixels). Pass 1 (window luma range and chroma
+//             hull) reads the horizontal table; pass 2 is specialized on the
+//             tap support so per-column terms stay in registers.
+//   luma resize       resampleH/V, resampleRadial src/kernels.cpp:171-334
+//   output store      floatToPlane src/lgcr.h:997-1013
 // FP64 accumulators stay FP64 (B200 issues FP64 at half the FP32 rate); a
 // product of two floats is exact in double, so fma(w, u, acc) rounds exactly
 // like the reference's acc += double(w) * u.
@@ -13,13 +23,284 @@
 
 namespace lgcr_b200 {
 
+// ---------------------------------------------------------------------------
+// horizontal table: hu hv mnU mxU | mnV mxV mnL mxL
+// ---------------------------------------------------------------------------
+template <int SUP>
+__device__ __forceinline__ void hpassAt(const FrameJob &J, int ox, int sy) {
+    const AxisView &ax = J.ax;
+    const int n = SUP > 0 ? SUP : ax.sup;
+    const int cw = J.cw;
+    const int tx0 = __ldg(ax.start + ox);
+    const double *wx = ax.wd + (size_t)ox * ax.sup;
+    const uint8_t *amx = ax.am + (size_t)ox * ax.sup;
+    const double2 *uv = reinterpret_cast<const double2 *>(J.uvd) + (size_t)sy * cw;
+    const float *lrow = J.lc ? J.lc + (size_t)sy * cw : nullptr;
+    double hU = 0.0, hV = 0.0;
+    double mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+    float mnL = 1e30f, mxL = -1e30f;
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+        if (__ldg(amx + i) == 0)
+            continue;
+        const int x = J.noClampX ? tx0 + i : iclamp(tx0 + i, 0, cw - 1);
+        const double2 p = __ldg(uv + x);
+        const double w = __ldg(wx + i);
+        hU = fma(w, p.x, hU);
+        hV = fma(w, p.y, hV);
+        mnU = smin(mnU, p.x); mxU = smax(mxU, p.x);
+        mnV = smin(mnV, p.y); mxV = smax(mxV, p.y);
+        if (lrow) {
+            const float l = ldf(lrow + x);
+            mnL = smin(mnL, l); mxL = smax(mxL, l);
+        }
+    }
+    float4 *o = reinterpret_cast<float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
+    o[0] = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
+    o[1] = make_float4((float)mnV, (float)mxV, mnL, mxL);
+}
+
+__global__ void __launch_bounds__(256)
+k_hpass(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, sy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, sy);
+    if (ox >= J.W || sy >= J.ch)
+        return;
+    switch (J.ax.sup) {
+    case 4: hpassAt<4>(J, ox, sy); break;
+    case 6: hpassAt<6>(J, ox, sy); break;
+    case 8: hpassAt<8>(J, ox, sy); break;
+    default: hpassAt<0>(J, ox, sy); break;
+    }
+}
+
+// Plain separable value from the horizontal table (vertical pass).
+template <int SUP>
+__device__ __forceinline__ void plainFromTableT(const FrameJob &J, int ox, int oy, float &outU,
+                                                float &outV) {
+    const AxisView &ax = J.ax, &ay = J.ay;
+    const int n = SUP > 0 ? SUP : ay.sup;
+    const int ty0 = __ldg(ay.start + oy);
+    const double *wy = ay.wd + (size_t)oy * ay.sup;
+    const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
+    double vU = 0.0, vV = 0.0;
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+        if (__ldg(amy + j) == 0)
+            continue;
+        const int sy = J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1);
+        const float4 *h = reinterpret_cast<const float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
+        const float4 a = __ldg(h), b = __ldg(h + 1);
+        const double w = __ldg(wy + j);
+        vU = fma(w, (double)a.x, vU);
+        vV = fma(w, (double)a.y, vV);
+        mnU = smin(mnU, a.z); mxU = smax(mxU, a.w);
+        mnV = smin(mnV, b.x); mxV = smax(mxV, b.y);
+    }
+    const double ws = (double)__ldg(ax.wsum + ox) * (double)__ldg(ay.wsum + oy);
+    const double wa = (double)__ldg(ax.wabs + ox) * (double)__ldg(ay.wabs + oy);
+    if (ws > 1e-6 && ws >= 0.05 * wa) {
+        vU /= ws;
+        vV /= ws;
+    } else {
+        const float px = __ldg(ax.pos + ox), py = __ldg(ay.pos + oy);
+        vU = bilinearAt(J.U, J.cw, J.ch, px, py);
+        vV = bilinearAt(J.V, J.cw, J.ch, px, py);
+    }
+    if (J.clampHull) {
+        vU = sclamp(vU, (double)(mnU - J.margin), (double)(mxU + J.margin));
+        vV = sclamp(vV, (double)(mnV - J.margin), (double)(mxV + J.margin));
+    }
+    outU = (float)vU;
+    outV = (float)vV;
+}
+
+__device__ __forceinline__ void plainFromTable(const FrameJob &J, int ox, int oy, float &u, float &v) {
+    switch (J.ay.sup) {
+    case 4: plainFromTableT<4>(J, ox, oy, u, v); break;
+    case 6: plainFromTableT<6>(J, ox, oy, u, v); break;
+    case 8: plainFromTableT<8>(J, ox, oy, u, v); break;
+    default: plainFromTableT<0>(J, ox, oy, u, v); break;
+    }
+}
+
 __device__ __forceinline__ void plainPixel(const FrameJob &J, int ox, int oy, float &u, float &v) {
-    plainAt(chromaPlainCtx(J), ox, oy, u, v);
+    if (!J.radial && J.kernel != 0 && J.hTab)
+        plainFromTable(J, ox, oy, u, v);
+    else
+        plainAt(chromaPlainCtx(J), ox, oy, u, v);
+}
+
+__device__ __forceinline__ bool pixelActive(const FrameJob &J, int ox, int oy) {
+    if (!J.sparse)
+        return true;
+    const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
+    const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
+    return J.mask[(size_t)my * J.sw + mx] != 0;
+}
+
+// Final sample of one output pixel: to the typed output plane when this
+// stage is the last one touching it, else to the float planes.
+__device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u, float v) {
+    if (J.directOutput) {
+        storeChroma(J, 1, ox, oy, u);
+        storeChroma(J, 2, ox, oy, v);
+    } else {
+        const size_t o = (size_t)oy * J.W + ox;
+        J.oU[o] = u;
+        J.oV[o] = v;
+    }
+}
+
+// Plain stage: every pixel the guided pass does not finalize.
+__global__ void __launch_bounds__(256)
+k_plain(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H)
+        return;
+    const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
+    // listed pixels of algo 2 and integer algo 4 are written by k_guided
+    if (J.listed && !floatSelector && pixelActive(J, ox, oy))
+        return;
+    float u, v;
+    plainPixel(J, ox, oy, u, v);
+    if (floatSelector) {
+        const size_t o = (size_t)oy * J.W + ox;
+        J.oU[o] = u;                    // base for the selector blend
+        J.oV[o] = v;
+        return;
+    }
+    emit(J, ox, oy, u, v);
 }
 
 // ---------------------------------------------------------------------------
-// guided reconstruction (algo 2; the algo 4 selector variants reuse it)
+// guided reconstruction
 // ---------------------------------------------------------------------------
+struct TapCtx {
+    const float *lc;
+    const double2 *uv;
+    int cw, ch;
+    float L0, nx, ny, scx, scy, rwF, rhF, invSigma2, guideFade, rescue, invG2, invG2Par;
+};
+
+struct Acc { double u, v, wsum, sumAbs; };
+
+__device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float dy_ny, float dy_nx,
+                                    float wx, Acc &a) {
+    const float dx = dxf * c.rwF;
+    const float dL = ldf(c.lc + o) - c.L0;
+    const float dp = dx * c.nx + dy_ny;
+    const float dt = -dx * c.ny + dy_nx;
+    const float simRaw = 1.0f / (1.0f + dL * dL * c.invSigma2);
+    const float sim = 1.0f - c.guideFade * (1.0f - simRaw);
+    const float bump = 1.0f / (1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par);
+    const float w = sim * (wx + c.rescue * bump);
+    const double wd = (double)w;
+    const double2 p = __ldg(c.uv + o);
+    a.u = fma(wd, p.x, a.u);
+    a.v = fma(wd, p.y, a.v);
+    a.wsum += wd;
+    a.sumAbs += fabs(wd);
+}
+
+// Separable base weights, all taps in range, support SUP (fully unrolled).
+template <int SUP>
+__device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
+                                              const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
+    float dxf[SUP], wxv[SUP];
+#pragma unroll
+    for (int i = 0; i < SUP; ++i) {
+        dxf[i] = (float)(tx0 + i) - c.scx;
+        wxv[i] = __ldg(wxp + i);
+    }
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((my >> j) & 1u))
+            continue;
+        const size_t rowOff = (size_t)(ty0 + j) * c.cw + tx0;
+        const float wy = __ldg(wyp + j);
+        const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
+        const float dy_ny = dy * c.ny, dy_nx = dy * c.nx;
+#pragma unroll
+        for (int i = 0; i < SUP; ++i) {
+            if (!((mx >> i) & 1u))
+                continue;
+            tap(c, rowOff + i, dxf[i], dy_ny, dy_nx, wxv[i] * wy, a);
+        }
+    }
+}
+
+// Any support, clamped taps; separable or radial base weights.
+__device__ __forceinline__ void tapsGeneric(const FrameJob &J, const TapCtx &c, int ox, int oy,
+                                            int tx0, int ty0, Acc &a) {
+    const AxisView &ax = J.ax, &ay = J.ay;
+    const float *wxp = ax.w + (size_t)ox * ax.sup;
+    const uint8_t *amx = ax.am + (size_t)ox * ax.sup;
+    const float *wyp = ay.w + (size_t)oy * ay.sup;
+    const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
+    const float *base = J.radial ? radialWeightsAt(J.rad, ox, oy) : nullptr;
+    for (int j = 0; j < ay.sup; ++j) {
+        if (__ldg(amy + j) == 0)
+            continue;
+        const size_t rowOff = (size_t)iclamp(ty0 + j, 0, c.ch - 1) * c.cw;
+        const float wy = __ldg(wyp + j);
+        const float dyf = (float)(ty0 + j) - c.scy;
+        const float dy = dyf * c.rhF;
+        const float dyc = dyf * J.invWyC;
+        const float dy_ny = dy * c.ny, dy_nx = dy * c.nx;
+        for (int i = 0; i < ax.sup; ++i) {
+            if (__ldg(amx + i) == 0)
+                continue;
+            const size_t o = rowOff + iclamp(tx0 + i, 0, c.cw - 1);
+            const float dxf = (float)(tx0 + i) - c.scx;
+            float wx;
+            if (base) {
+                wx = ldf(base + (size_t)j * ax.sup + i);
+            } else if (J.radial) {
+                const float dxc = dxf * J.invWxC;
+                wx = lutLookupDev(J.lut, J.lutN, sqrtf(dxc * dxc + dyc * dyc) * J.lutScale);
+            } else {
+                wx = __ldg(wxp + i) * wy;
+            }
+            tap(c, o, dxf, dy_ny, dy_nx, wx, a);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t maskBits(const uint8_t *am, int n) {
+    uint32_t m = 0;
+    for (int i = 0; i < n; ++i)
+        m |= (__ldg(am + i) != 0 ? 1u : 0u) << i;
+    return m;
+}
+
+// Window extrema of U, V and lc over the active taps from the table rows:
+// ext = {minU, maxU, minV, maxV, minL, maxL}.
+template <int SUP>
+__device__ __forceinline__ void windowExtrema(const FrameJob &J, int ox, int ty0, const uint8_t *amy,
+                                              float *ext) {
+    const int n = SUP > 0 ? SUP : J.ay.sup;
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f, mnL = 1e30f, mxL = -1e30f;
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+        if (__ldg(amy + j) == 0)
+            continue;
+        const int sy = J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1);
+        const float4 *h = reinterpret_cast<const float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
+        const float4 a = __ldg(h), b = __ldg(h + 1);
+        mnU = smin(mnU, a.z); mxU = smax(mxU, a.w);
+        mnV = smin(mnV, b.x); mxV = smax(mxV, b.y);
+        mnL = smin(mnL, b.z); mxL = smax(mxL, b.w);
+    }
+    ext[0] = mnU; ext[1] = mxU; ext[2] = mnV; ext[3] = mxV; ext[4] = mnL; ext[5] = mxL;
+}
+
 struct Guided {
     double u, v;
     float L0, ssRamp, guideFade, nx, ny;
@@ -77,7 +358,9 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
         mutualFade = 1.0f - J.msStrength * (1.0f - gate);
     }
 
-    // pass 1: window luma range and chroma hull over active taps
+    // pass 1: window luma range and chroma hull over the active taps. The
+    // luma range max|lc - L0| equals max(|max lc - L0|, |min lc - L0|)
+    // exactly (float subtraction is monotonic), so the table's extrema serve.
     const int tx0 = __ldg(ax.start + ox), ty0 = __ldg(ay.start + oy);
     const float *wxp = ax.w + (size_t)ox * ax.sup;
     const uint8_t *amx = ax.am + (size_t)ox * ax.sup;
@@ -85,18 +368,31 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
     float maxAbsDL = 0.0f;
     float hMinU = 1e30f, hMaxU = -1e30f, hMinV = 1e30f, hMaxV = -1e30f;
-    for (int j = 0; j < ay.sup; ++j) {
-        if (__ldg(amy + j) == 0)
-            continue;
-        const size_t rowOff = (size_t)iclamp(ty0 + j, 0, ch - 1) * cw;
-        for (int i = 0; i < ax.sup; ++i) {
-            if (__ldg(amx + i) == 0)
+    if (!J.radial && J.hTab) {
+        float ext[6];
+        switch (ay.sup) {
+        case 4: windowExtrema<4>(J, ox, ty0, amy, ext); break;
+        case 6: windowExtrema<6>(J, ox, ty0, amy, ext); break;
+        case 8: windowExtrema<8>(J, ox, ty0, amy, ext); break;
+        default: windowExtrema<0>(J, ox, ty0, amy, ext); break;
+        }
+        hMinU = ext[0]; hMaxU = ext[1]; hMinV = ext[2]; hMaxV = ext[3];
+        maxAbsDL = smax(maxAbsDL, fabsf(ext[5] - L0));
+        maxAbsDL = smax(maxAbsDL, fabsf(ext[4] - L0));
+    } else {
+        for (int j = 0; j < ay.sup; ++j) {
+            if (__ldg(amy + j) == 0)
                 continue;
-            const size_t o = rowOff + iclamp(tx0 + i, 0, cw - 1);
-            const float l = ldf(J.lc + o), u = ldf(J.U + o), v = ldf(J.V + o);
-            maxAbsDL = smax(maxAbsDL, fabsf(l - L0));
-            hMinU = smin(hMinU, u); hMaxU = smax(hMaxU, u);
-            hMinV = smin(hMinV, v); hMaxV = smax(hMaxV, v);
+            const size_t rowOff = (size_t)iclamp(ty0 + j, 0, ch - 1) * cw;
+            for (int i = 0; i < ax.sup; ++i) {
+                if (__ldg(amx + i) == 0)
+                    continue;
+                const size_t o = rowOff + iclamp(tx0 + i, 0, cw - 1);
+                const float l = ldf(J.lc + o), u = ldf(J.U + o), v = ldf(J.V + o);
+                maxAbsDL = smax(maxAbsDL, fabsf(l - L0));
+                hMinU = smin(hMinU, u); hMaxU = smax(hMaxU, u);
+                hMinV = smin(hMinV, v); hMaxV = smax(hMaxV, v);
+            }
         }
     }
 
@@ -180,52 +476,32 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
         }
     }
     const float aniso = 1.0f + J.stretch * dir.coherence;
-    const float invG2 = J.invGsigma2;
-    const float invG2Par = invG2 / (aniso * aniso);
 
-    // pass 2: sup x sup taps with w = sim * (wbase + rescue * bump)
-    double accU = 0.0, accV = 0.0, wsum = 0.0, sumAbs = 0.0;
-    const float *base = J.radial ? radialWeightsAt(J.rad, ox, oy) : nullptr;
-    for (int j = 0; j < ay.sup; ++j) {
-        if (__ldg(amy + j) == 0)
-            continue;
-        const size_t rowOff = (size_t)iclamp(ty0 + j, 0, ch - 1) * cw;
-        const float wy = __ldg(wyp + j);
-        const float dyf = (float)(ty0 + j) - scy;
-        const float dy = dyf * J.rhF;
-        const float dyc = dyf * J.invWyC;
-        for (int i = 0; i < ax.sup; ++i) {
-            if (__ldg(amx + i) == 0)
-                continue;
-            const size_t o = rowOff + iclamp(tx0 + i, 0, cw - 1);
-            const float dxf = (float)(tx0 + i) - scx;
-            float wx;
-            if (base)
-                wx = ldf(base + (size_t)j * ax.sup + i);
-            else if (J.radial) {
-                const float dxc = dxf * J.invWxC;
-                wx = lutLookupDev(J.lut, J.lutN, sqrtf(dxc * dxc + dyc * dyc) * J.lutScale);
-            } else
-                wx = __ldg(wxp + i) * wy;
-            const float dx = dxf * J.rwF;
-            const float dL = ldf(J.lc + o) - L0;
-            const float dp = dx * nx + dy * ny;
-            const float dt = -dx * ny + dy * nx;
-            const float simRaw = 1.0f / (1.0f + dL * dL * invSigma2);
-            const float sim = 1.0f - guideFade * (1.0f - simRaw);
-            const float bump = 1.0f / (1.0f + dp * dp * invG2 + dt * dt * invG2Par);
-            const float w = sim * (wx + rescue * bump);
-            const double wd = (double)w;
-            accU = fma(wd, (double)ldf(J.U + o), accU);
-            accV = fma(wd, (double)ldf(J.V + o), accV);
-            wsum += wd;
-            sumAbs += (double)fabsf(w);
-        }
-    }
+    // pass 2: taps with w = sim * (wbase + rescue * bump)
+    TapCtx c;
+    c.lc = J.lc;
+    c.uv = reinterpret_cast<const double2 *>(J.uvd);
+    c.cw = cw; c.ch = ch;
+    c.L0 = L0; c.nx = nx; c.ny = ny; c.scx = scx; c.scy = scy;
+    c.rwF = J.rwF; c.rhF = J.rhF;
+    c.invSigma2 = invSigma2; c.guideFade = guideFade; c.rescue = rescue;
+    c.invG2 = J.invGsigma2;
+    c.invG2Par = J.invGsigma2 / (aniso * aniso);
+    Acc a{0.0, 0.0, 0.0, 0.0};
+    const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup;
+    if (fast && ax.sup == 8)
+        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
+    else if (fast && ax.sup == 6)
+        tapsSeparable<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
+    else if (fast && ax.sup == 4)
+        tapsSeparable<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
+    else
+        tapsGeneric(J, c, ox, oy, tx0, ty0, a);
+
     double valueU, valueV;
-    if (wsum > 1e-6 && wsum >= 0.05 * sumAbs) {
-        valueU = accU / wsum;
-        valueV = accV / wsum;
+    if (a.wsum > 1e-6 && a.wsum >= 0.05 * a.sumAbs) {
+        valueU = a.u / a.wsum;
+        valueV = a.v / a.wsum;
     } else {
         valueU = bilinearAt(J.U, cw, ch, scx, scy);
         valueV = bilinearAt(J.V, cw, ch, scx, scy);
@@ -245,80 +521,23 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     return g;
 }
 
-__device__ __forceinline__ bool pixelActive(const FrameJob &J, int ox, int oy) {
-    if (!J.sparse)
-        return true;
-    const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
-    const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
-    return J.mask[(size_t)my * J.sw + mx] != 0;
-}
-
-// Final sample of one output pixel: to the typed output plane when this
-// stage is the last one touching it, else to the float planes.
-__device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u, float v) {
-    if (J.directOutput) {
-        storeChroma(J, 1, ox, oy, u);
-        storeChroma(J, 2, ox, oy, v);
-    } else {
-        const size_t o = (size_t)oy * J.W + ox;
-        J.oU[o] = u;
-        J.oV[o] = v;
-    }
-}
-
-__global__ void __launch_bounds__(256)
-k_recon(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
-    int ox, oy;
-    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
-    if (ox >= J.W || oy >= J.H)
-        return;
-    if (!J.guided) {                                   // strength == 0: plain only
-        float u, v;
-        plainPixel(J, ox, oy, u, v);
-        emit(J, ox, oy, u, v);
-        return;
-    }
+// One listed pixel: algo 2 output, or the algo 4 selector (recon.cpp:762-811).
+__device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy) {
+    const Guided g = guidedPixel(J, ox, oy);
     if (J.algo == 2) {
-        const bool active = pixelActive(J, ox, oy);
-        if (!active) {                                 // sparse: plain kernel suffices
-            float u, v;
-            plainPixel(J, ox, oy, u, v);
-            emit(J, ox, oy, u, v);
-            return;
-        }
-        const Guided g = guidedPixel(J, ox, oy);
         emit(J, ox, oy, (float)g.u, (float)g.v);
         return;
     }
-    if (J.algo == 6) {                                 // plain base; detail later
-        float u, v;
-        plainPixel(J, ox, oy, u, v);
-        emit(J, ox, oy, u, v);
-        return;
-    }
-    // algo 4: plain base plus guided routing (recon.cpp:762-811)
-    float baseU, baseV;
-    plainPixel(J, ox, oy, baseU, baseV);
-    const size_t o = (size_t)oy * J.W + ox;
-    if (!pixelActive(J, ox, oy)) {
-        if (J.outKind == kF32) {
-            J.oU[o] = baseU;
-            J.oV[o] = baseV;
-        } else {
-            emit(J, ox, oy, baseU, baseV);
-        }
-        return;
-    }
-    const Guided g = guidedPixel(J, ox, oy);
     const float diag = g.hasDir ? smin(1.0f, 2.0f * fabsf(g.nx * g.ny)) : 0.0f;
     const float hedgy = (1.0f - g.ssRamp) * g.guideFade;
     const float sel = J.strength4;
     const float w2 = hedgy * (1.0f - diag) * sel;
     const float w3 = hedgy * diag * sel;
+    const size_t o = (size_t)oy * J.W + ox;
     if (J.outKind != kF32) {
-        // integer output: single-expression fused selector
+        // integer output: single-expression fused selector on the plain base
+        float baseU, baseV;
+        plainPixel(J, ox, oy, baseU, baseV);
         double valueU, valueV;
         if (w2 >= 1e-4f || w3 >= 1e-4f) {
             const int cx = __ldg(J.ax.cbI0 + ox), cy = __ldg(J.ay.cbI0 + oy);
@@ -340,8 +559,7 @@ k_recon(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, in
         return;
     }
     // float output: routing metadata; blended after the ROI-limited LGF
-    J.oU[o] = baseU;
-    J.oV[o] = baseV;
+    const float baseU = J.oU[o], baseV = J.oV[o];
     const bool compressed = J.sparse &&
         (unsigned long long)J.counters[kCntActiveOutput] * 2ull < (unsigned long long)J.W * J.H;
     if (compressed) {
@@ -360,6 +578,57 @@ k_recon(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, in
         J.selW2[o] = hedgy * (1.0f - diag);
         J.selW3[o] = hedgy * diag;
     }
+}
+
+// Persistent grid over the work lists of all frames in the launch. Each
+// block builds the prefix of the frames' list lengths in shared memory and
+// strides over the concatenated work.
+constexpr int kGuidedMaxFrames = 1024;
+
+template <int MIN_BLOCKS>
+__device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, int njobs) {
+    __shared__ unsigned long long pre[kGuidedMaxFrames + 1];
+    for (int chunk = 0; chunk < njobs; chunk += kGuidedMaxFrames) {
+        const int n = min(kGuidedMaxFrames, njobs - chunk);
+        if (threadIdx.x == 0) {
+            unsigned long long acc = 0;
+            for (int i = 0; i < n; ++i) {
+                pre[i] = acc;
+                const FrameJob &J = jobs[chunk + i];
+                if (J.listed)
+                    acc += J.counters[kCntActiveOutput];
+            }
+            pre[n] = acc;
+        }
+        __syncthreads();
+        const unsigned long long total = pre[n];
+        for (unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+             w += (unsigned long long)gridDim.x * blockDim.x) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pre[mid] <= w) lo = mid; else hi = mid - 1;
+            }
+            const FrameJob &J = jobs[chunk + lo];
+            const uint32_t pix = J.actList[w - pre[lo]];
+            guidedWork(J, (int)(pix & 0xffffu), (int)(pix >> 16));
+        }
+        __syncthreads();
+    }
+}
+
+// Two register budgets of the same persistent kernel: 2 resident blocks per
+// SM (no spills) or 3 (fewer registers, a few spills); the autotuner picks.
+__global__ void __launch_bounds__(256, 2)
+k_guided(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 3)
+k_guided3(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<3>(jobs, njobs);
 }
 
 // Float output planes -> typed output (output conversion stage).

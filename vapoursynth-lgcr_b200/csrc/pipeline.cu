@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace lgcr_b200 {
@@ -213,12 +214,13 @@ struct Packer {
     }
 };
 
-struct AxisOffsets { size_t start, w, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF; int n, sup; };
+struct AxisOffsets { size_t start, w, wd, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF; int n, sup; };
 
 AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
     AxisOffsets o;
     o.n = a.n; o.sup = a.sup;
-    o.start = pk.add(a.start); o.w = pk.add(a.w); o.am = pk.add(a.am);
+    const std::vector<double> wd(a.w.begin(), a.w.end());
+    o.start = pk.add(a.start); o.w = pk.add(a.w); o.wd = pk.add(wd); o.am = pk.add(a.am);
     o.wsum = pk.add(a.weightSum); o.wabs = pk.add(a.absoluteWeightSum);
     o.pos = pk.add(a.pos); o.lpos = pk.add(a.lpos);
     o.cbI0 = pk.add(a.chromaBilin.i0); o.cbF = pk.add(a.chromaBilin.f);
@@ -230,6 +232,7 @@ AxisView axisView(const DeviceArena &ar, const AxisOffsets &o) {
     AxisView v;
     v.n = o.n; v.sup = o.sup;
     v.start = (const int *)ar.at(o.start); v.w = (const float *)ar.at(o.w);
+    v.wd = (const double *)ar.at(o.wd);
     v.am = (const uint8_t *)ar.at(o.am); v.wsum = (const float *)ar.at(o.wsum);
     v.wabs = (const float *)ar.at(o.wabs); v.pos = (const float *)ar.at(o.pos);
     v.lpos = (const float *)ar.at(o.lpos); v.cbI0 = (const int *)ar.at(o.cbI0);
@@ -421,10 +424,14 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     Slot sOU = take(O * 4), sOV = take(O * 4);
     Slot sLumaTmp = take(size_t(p.outW) * sh * 4, !sameSize && !p.k.radial);  // luma / detail resize
     Slot sCnt = take(kCntCount * sizeof(unsigned long long));
+    const bool listed = guided && (p.algo == 2 || p.algo == 4);
+    Slot sUvd = take(C * 16), sHTab = take(size_t(p.outW) * ch * 32, !p.k.radial);
+    Slot sList = take(O * 4, listed);
     const bool algo6 = guided && p.algo == 6, algo4 = guided && p.algo == 4;
     Slot sAff = take(9 * C * 4, algo6), sYc1 = take(C * 4, algo6), sYc2 = take(C * 4, algo6);
     Slot sDt1 = take(L * 4, algo6), sDt2 = take(L * 4, algo6);
     Slot sDet = take(O * 4, algo6 && !sameSize);
+    Slot sDTab = take(size_t(sw) * ch * 16, algo6 && !p.k.radial && p.k.kernel != Kernel::Bilinear);
     Slot sLumaTmp2 = take(size_t(p.outW) * sh * 4, algo6 && !sameSize && !p.k.radial && false);
     Slot sLgf = take(6 * C * 4, algo4);
     const bool sel = algo4 && isFloat();
@@ -449,8 +456,11 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     ws->seed = B(sSeed); ws->mtmp = B(sMtmp); ws->mask = B(sMask); ws->cmask = B(sCmask);
     ws->oU = F(sOU); ws->oV = F(sOV); ws->lumaTmp = F(sLumaTmp);
     ws->counters = (unsigned long long *)ar.at(sCnt.off);
+    ws->uvd = sUvd.on ? (double *)ar.at(sUvd.off) : nullptr;
+    ws->hTab = F(sHTab);
+    ws->actList = sList.on ? (uint32_t *)ar.at(sList.off) : nullptr;
     ws->aff = F(sAff); ws->yc1 = F(sYc1); ws->yc2 = F(sYc2);
-    ws->detailTmp = F(sDt1); ws->detailTmp2 = F(sDt2); ws->detail = F(sDet);
+    ws->detailTmp = F(sDt1); ws->detailTmp2 = F(sDt2); ws->detail = F(sDet); ws->dTab = F(sDTab);
     (void)sLumaTmp2;
     ws->lgf = F(sLgf);
     ws->selW2 = F(sW2); ws->selW3 = F(sW3); ws->gU = F(sGU); ws->gV = F(sGV);
@@ -597,9 +607,21 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.seed = ws.seed; J.mtmp = ws.mtmp; J.mask = ws.mask; J.cmask = ws.cmask;
     J.oU = ws.oU; J.oV = ws.oV; J.lumaTmp = ws.lumaTmp;
     J.counters = ws.counters;
+    J.uvd = ws.uvd;
+    J.hTab = ws.hTab;
+    J.actList = ws.actList;
+    J.listed = J.guided && (p.algo == 2 || p.algo == 4);
+    {
+        // every tap index in range: starts lie in [0, srcChromaN - sup] and the
+        // integer-ratio chroma count equals the plane size
+        const int nx = (F.sw + int(J.rw) - 1) / int(J.rw);
+        const int ny = (F.sh + int(J.rh) - 1) / int(J.rh);
+        J.noClampX = (nx == F.cw && F.cw >= T.axSup) ? 1 : 0;
+        J.noClampY = (ny == F.ch && F.ch >= T.aySup) ? 1 : 0;
+    }
     // algo 6
     J.aff = ws.aff; J.yc1 = ws.yc1; J.yc2 = ws.yc2;
-    J.detailTmp = ws.detailTmp; J.detailTmp2 = ws.detailTmp2;
+    J.detailTmp = ws.detailTmp; J.detailTmp2 = ws.detailTmp2; J.dTab = ws.dTab;
     J.ycH1 = T.ycH1; J.ycV1 = T.ycV1; J.ycH2 = T.ycH2; J.ycV2 = T.ycV2;
     J.sax = T.sax; J.say = T.say; J.srad = T.srad;
     J.nyqX = T.nyqX; J.nyqY = T.nyqY;
@@ -631,8 +653,8 @@ void buildJob(const FrameTask &t, FrameJob &J) {
 // ---------------------------------------------------------------------------
 enum StageId : int {
     S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_LC, S_DIL_H, S_DIL_V,
-    S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_RECON,
-    S_YC, S_AFFINE, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
+    S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
+    S_YC, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
     S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
@@ -646,7 +668,7 @@ const char *stageName(int s) {
         "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
         "buildGuideMaps_tensor", "buildGuideMaps_lc", "buildTrustMask_h", "buildTrustMask_v",
         "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
-        "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_plain",
+        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain",
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
         "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
         "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
@@ -671,7 +693,7 @@ static void initShapes() {
 }
 
 bool stageTunable(int s) {
-    return s == S_RECON || s == S_AFFINE || s == S_DET_TRANSFER || s == S_DET_PLAIN ||
+    return s == S_PLAIN || s == S_HPASS || s == S_AFFINE || s == S_DET_TRANSFER || s == S_DET_PLAIN ||
            s == S_LGF_DENSE || s == S_YC || s == S_BM_AGG;
 }
 
@@ -687,6 +709,24 @@ void setStageShape(int s, int bx, int by) {
     gShapeX[s] = bx; gShapeY[s] = by;
 }
 
+// Register-budget variant of the persistent guided kernel (0: 2 blocks/SM,
+// 1: 3 blocks/SM). LGCR_GUIDED_VARIANT sets the initial choice.
+static int gGuidedVariant = -1;
+
+int guidedVariant() {
+    std::lock_guard<std::mutex> lock(gShapeMu);
+    if (gGuidedVariant < 0) {
+        const char *e = std::getenv("LGCR_GUIDED_VARIANT");
+        gGuidedVariant = (e && e[0] == '1') ? 1 : 0;
+    }
+    return gGuidedVariant;
+}
+
+void setGuidedVariant(int v) {
+    std::lock_guard<std::mutex> lock(gShapeMu);
+    gGuidedVariant = v ? 1 : 0;
+}
+
 static int stageTilesShaped(const FrameJob &J, int s);
 
 static int stageTiles(const FrameJob &J, int s) {
@@ -696,7 +736,8 @@ static int stageTiles(const FrameJob &J, int s) {
         int bx, by;
         stageShape(s, bx, by);
         switch (s) {
-        case S_RECON: case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
+        case S_PLAIN: case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
+        case S_HPASS: return cdiv(J.W, bx) * cdiv(J.ch, by);
         case S_AFFINE: case S_LGF_DENSE: case S_YC: return cdiv(J.cw, bx) * cdiv(J.ch, by);
         case S_DET_PLAIN: return cdiv(J.sw, bx) * cdiv(J.sh, by);
         }
@@ -719,13 +760,16 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_LC: return J.guided ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_DIL_H: return J.sparse ? cdiv(J.sw, 1024) * J.sh : 0;
     case S_DIL_V: return J.sparse ? cdiv(J.sw, 32) * cdiv(J.sh, 128) : 0;
-    case S_MARK: return J.sparse ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_MARK: return (J.sparse || J.listed) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_COUNT: return J.sparse ? cdiv(J.sw * J.sh, 1024) : 0;
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_RECON: return cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_HPASS: return (J.hTab && !J.radial && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
+    case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC:
     case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_PLAIN: return (J.guided && J.algo == 6) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_RH: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_RV: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
@@ -790,9 +834,28 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_COUNT, k_count, dim3(256));
     go(S_GATE, k_gate, b32x8);
     go(S_LGF_DENSE, k_lgf, b32x8);
-    go(S_RECON, k_recon, b32x8);
+    go(S_HPASS, k_hpass, b32x8);
+    go(S_PLAIN, k_plain, b32x8);
+    if (plan.totals[S_GUIDED] > 0) {
+        // persistent grid: enough resident blocks to fill every SM
+        const int variant = guidedVariant();
+        static int gridBlocks[2] = {0, 0};
+        if (gridBlocks[variant] == 0) {
+            int dev = 0, sms = 0, perSm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, variant ? k_guided3 : k_guided, 256, 0);
+            gridBlocks[variant] = std::max(1, sms * std::max(1, perSm));
+        }
+        if (variant)
+            k_guided3<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
+        else
+            k_guided<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
+        ++launches;
+    }
     go(S_YC, k_yc_h, b32x8);
     go(S_AFFINE, k_affine, b32x8);
+    go(S_DET_HPASS, k_detail_hpass, b32x8);
     go(S_DET_PLAIN, k_detail_plain, b32x8);
     for (int pass = 0; pass < 8; ++pass) {
         const int s = S_NYQ0 + pass;

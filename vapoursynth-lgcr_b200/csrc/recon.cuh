@@ -27,6 +27,7 @@ struct AxisView {
     int n, sup;
     const int *start;
     const float *w;          // n * sup
+    const double *wd;        // n * sup, the same weights in FP64
     const uint8_t *am;       // n * sup
     const float *wsum, *wabs;
     const float *pos, *lpos;
@@ -103,12 +104,18 @@ struct FrameJob {
     float *oU, *oV;                    // W x H float output planes
     float *lumaTmp;                    // W x sh luma resize intermediate
     unsigned long long *counters;      // kCntCount
+    float *hTab;                       // W x ch x 8: horizontal sums + window extrema
+    double *uvd;                       // cw x ch x 2: (u, v) in FP64
+    uint32_t *actList;                 // active output pixels (y << 16 | x)
+    int listed;                        // frame uses the guided work list
+    int noClampX, noClampY;            // every chroma tap index is in range
     // algo 6 / algo 4 / bm workspaces
     float *aff;                        // 9 chroma planes: aU aV g mnU mxU mnV mxV rng dgl
     float *yc1, *yc2;                  // bilinear / bicubic degradation candidates
     float *ycTmp;                      // cw x sh candidate intermediate (resize case)
     float *detail;                     // sw x sh (or W x H) detail map
     float *detailTmp, *detailTmp2;     // sw x sh scratch
+    float *dTab;                       // sw x ch x 4: degraded-luma horizontal pass
     WeightView ycH1, ycV1, ycH2, ycV2; // candidate degradation tables
     WeightView detH, detV;             // detail resample to output (resize)
     int nyqX, nyqY;                    // dyadic Nyquist passes per axis

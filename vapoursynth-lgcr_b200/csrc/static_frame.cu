@@ -106,11 +106,12 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     const ChromaAxis ax = buildChromaAxis(F.sw, q.outW, rw, q.shiftX, q.k);
     const ChromaAxis ay = buildChromaAxis(F.sh, q.outH, rh, q.shiftY, q.k);
     Image img;
-    struct AxisOff { size_t s, w, am, ws, wa, pos, lpos, ci, cf, li, lf; } oa[2];
+    struct AxisOff { size_t s, w, wd, am, ws, wa, pos, lpos, ci, cf, li, lf; } oa[2];
     const ChromaAxis *axes[2] = { &ax, &ay };
     for (int i = 0; i < 2; ++i) {
         const ChromaAxis &a = *axes[i];
-        oa[i] = { img.add(a.start), img.add(a.w), img.add(a.am), img.add(a.weightSum),
+        const std::vector<double> wd(a.w.begin(), a.w.end());
+        oa[i] = { img.add(a.start), img.add(a.w), img.add(wd), img.add(a.am), img.add(a.weightSum),
                   img.add(a.absoluteWeightSum), img.add(a.pos), img.add(a.lpos),
                   img.add(a.chromaBilin.i0), img.add(a.chromaBilin.f),
                   img.add(a.lumaBilin.i0), img.add(a.lumaBilin.f) };
@@ -152,6 +153,8 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     const size_t oSeed = sparse ? take(L) : 0, oMtmp = sparse ? take(L) : 0;
     const size_t oMask = sparse ? take(L) : 0, oCmask = sparse ? take(C) : 0;
     const size_t oLumaTmp = (!sameSize && !q.k.radial) ? take(size_t(q.outW) * F.sh * 4) : 0;
+    const size_t oUvd = take(C * 16);
+    const size_t oList = guided ? take(size_t(q.outW) * q.outH * 4) : 0;
     if (cursor > kStaticScratchBytes) {
         char msg[200];
         std::snprintf(msg, sizeof(msg),
@@ -166,6 +169,7 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
         AxisView v;
         v.n = a.n; v.sup = a.sup;
         v.start = (const int *)(base + o.s); v.w = (const float *)(base + o.w);
+        v.wd = (const double *)(base + o.wd);
         v.am = (const uint8_t *)(base + o.am); v.wsum = (const float *)(base + o.ws);
         v.wabs = (const float *)(base + o.wa); v.pos = (const float *)(base + o.pos);
         v.lpos = (const float *)(base + o.lpos); v.cbI0 = (const int *)(base + o.ci);
@@ -203,6 +207,9 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     ws.mask = sparse ? bp(oMask) : nullptr; ws.cmask = sparse ? bp(oCmask) : nullptr;
     ws.lumaTmp = oLumaTmp ? fp(oLumaTmp) : nullptr;
     ws.counters = (unsigned long long *)(base + oCnt);
+    ws.uvd = (double *)(base + oUvd);
+    ws.actList = guided ? (uint32_t *)(base + oList) : nullptr;
+    ws.hTab = nullptr;      // plain and guided windows are read directly
 
     FrameTask t;
     t.filter = &F;
