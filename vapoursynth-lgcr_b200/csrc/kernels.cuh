@@ -9,6 +9,11 @@ namespace lgcr_b200 {
 
 #define LGCR_STAGE_ARGS const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs
 
+// k_plain: output rows per block (32 columns wide, 32x8 threads) and the
+// most horizontal-table rows one block stages in shared memory.
+constexpr int kPlainRows = 32;
+constexpr int kPlainStagedRows = 40;
+
 __global__ void k_convert(LGCR_STAGE_ARGS);
 __global__ void k_tensor(LGCR_STAGE_ARGS);
 __global__ void k_lc(LGCR_STAGE_ARGS);

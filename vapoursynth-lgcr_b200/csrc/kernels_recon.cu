@@ -155,28 +155,120 @@ __device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u,
     }
 }
 
-// Plain stage: every pixel the guided pass does not finalize.
+// Vertical pass over table rows staged in shared memory: same arithmetic and
+// order as plainFromTableT, rows indexed relative to the staged block.
+template <int SUP>
+__device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 (*sHV)[32],
+                                                const float2 (*sU)[32], const float2 (*sV)[32],
+                                                int syLo, int lx, int ox, int oy, float &outU,
+                                                float &outV) {
+    const AxisView &ax = J.ax, &ay = J.ay;
+    const int n = SUP > 0 ? SUP : ay.sup;
+    const int ty0 = __ldg(ay.start + oy);
+    const double *wy = ay.wd + (size_t)oy * ay.sup;
+    const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
+    double vU = 0.0, vV = 0.0;
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+        if (__ldg(amy + j) == 0)
+            continue;
+        const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
+        const float2 h = sHV[r][lx], eu = sU[r][lx], ev = sV[r][lx];
+        const double w = __ldg(wy + j);
+        vU = fma(w, (double)h.x, vU);
+        vV = fma(w, (double)h.y, vV);
+        mnU = smin(mnU, eu.x); mxU = smax(mxU, eu.y);
+        mnV = smin(mnV, ev.x); mxV = smax(mxV, ev.y);
+    }
+    const double ws = (double)__ldg(ax.wsum + ox) * (double)__ldg(ay.wsum + oy);
+    const double wa = (double)__ldg(ax.wabs + ox) * (double)__ldg(ay.wabs + oy);
+    if (ws > 1e-6 && ws >= 0.05 * wa) {
+        vU /= ws;
+        vV /= ws;
+    } else {
+        const float px = __ldg(ax.pos + ox), py = __ldg(ay.pos + oy);
+        vU = bilinearAt(J.U, J.cw, J.ch, px, py);
+        vV = bilinearAt(J.V, J.cw, J.ch, px, py);
+    }
+    if (J.clampHull) {
+        vU = sclamp(vU, (double)(mnU - J.margin), (double)(mxU + J.margin));
+        vV = sclamp(vV, (double)(mnV - J.margin), (double)(mxV + J.margin));
+    }
+    outU = (float)vU;
+    outV = (float)vV;
+}
+
+// Plain stage: every pixel the guided pass does not finalize. A block covers
+// 32 output columns x kPlainRows output rows; for the separable table path
+// it first stages the table rows its windows touch (each row read once per
+// block instead of once per output pixel), then runs the vertical pass from
+// shared memory. Blocks whose rows do not fit (strong vertical downscale)
+// read the table directly.
 __global__ void __launch_bounds__(256)
 k_plain(LGCR_STAGE_ARGS) {
+    __shared__ float2 sHV[kPlainStagedRows][32];
+    __shared__ float2 sU[kPlainStagedRows][32];
+    __shared__ float2 sV[kPlainStagedRows][32];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
-    int ox, oy;
-    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
-    if (ox >= J.W || oy >= J.H)
+    const int tile = blockIdx.x - tileStart[f];
+    const int tilesX = (J.W + 31) >> 5;
+    const int colBase = (tile % tilesX) * 32;
+    const int oy0 = (tile / tilesX) * kPlainRows;
+    const int lx = threadIdx.x;
+    const int ox = colBase + lx;
+    const bool table = !J.radial && J.kernel != 0 && J.hTab;
+    int syLo = 0, nRows = 0;
+    if (table) {
+        const int oyLast = min(oy0 + kPlainRows, J.H) - 1;
+        syLo = iclamp(__ldg(J.ay.start + oy0), 0, J.ch - 1);
+        const int syHi = iclamp(__ldg(J.ay.start + oyLast) + J.ay.sup - 1, 0, J.ch - 1);
+        nRows = syHi - syLo + 1;
+    }
+    const bool staged = table && nRows <= kPlainStagedRows;
+    if (staged) {
+        if (ox < J.W) {
+            for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
+                const float4 *h =
+                    reinterpret_cast<const float4 *>(J.hTab + ((size_t)(syLo + r) * J.W + ox) * 8);
+                const float4 a = __ldg(h), b = __ldg(h + 1);
+                sHV[r][lx] = make_float2(a.x, a.y);
+                sU[r][lx] = make_float2(a.z, a.w);
+                sV[r][lx] = make_float2(b.x, b.y);
+            }
+        }
+        __syncthreads();
+    }
+    if (ox >= J.W)
         return;
     const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
-    // listed pixels of algo 2 and integer algo 4 are written by k_guided
-    if (J.listed && !floatSelector && pixelActive(J, ox, oy))
-        return;
-    float u, v;
-    plainPixel(J, ox, oy, u, v);
-    if (floatSelector) {
-        const size_t o = (size_t)oy * J.W + ox;
-        J.oU[o] = u;                    // base for the selector blend
-        J.oV[o] = v;
-        return;
+    for (int k = threadIdx.y; k < kPlainRows; k += blockDim.y) {
+        const int oy = oy0 + k;
+        if (oy >= J.H)
+            break;
+        // listed pixels of algo 2 and integer algo 4 are written by k_guided
+        if (J.listed && !floatSelector && pixelActive(J, ox, oy))
+            continue;
+        float u, v;
+        if (staged) {
+            switch (J.ay.sup) {
+            case 4: plainFromStaged<4>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
+            case 6: plainFromStaged<6>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
+            case 8: plainFromStaged<8>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
+            default: plainFromStaged<0>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
+            }
+        } else {
+            plainPixel(J, ox, oy, u, v);
+        }
+        if (floatSelector) {
+            const size_t o = (size_t)oy * J.W + ox;
+            J.oU[o] = u;                    // base for the selector blend
+            J.oV[o] = v;
+            continue;
+        }
+        emit(J, ox, oy, u, v);
     }
-    emit(J, ox, oy, u, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -191,49 +283,70 @@ struct TapCtx {
 
 struct Acc { double u, v, wsum, sumAbs; };
 
-__device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float dy_ny, float dy_nx,
-                                    float wx, Acc &a) {
-    const float dx = dxf * c.rwF;
-    const float dL = ldf(c.lc + o) - c.L0;
-    const float dp = dx * c.nx + dy_ny;
-    const float dt = -dx * c.ny + dy_nx;
+// One tap of pass 2 (recon.cpp:606-623). dxnx = dx*nx and dxny = (-dx)*ny
+// are the per-column products of the reference's dp and dt, hoisted out of
+// the row loop (same operands, same rounding).
+__device__ __forceinline__ void tapCore(const TapCtx &c, float l, double2 p, float dxnx, float dxny,
+                                        float dy_ny, float dy_nx, float wx, Acc &a) {
+    const float dL = l - c.L0;
+    const float dp = dxnx + dy_ny;
+    const float dt = dxny + dy_nx;
     const float simRaw = 1.0f / (1.0f + dL * dL * c.invSigma2);
     const float sim = 1.0f - c.guideFade * (1.0f - simRaw);
     const float bump = 1.0f / (1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par);
     const float w = sim * (wx + c.rescue * bump);
     const double wd = (double)w;
-    const double2 p = __ldg(c.uv + o);
     a.u = fma(wd, p.x, a.u);
     a.v = fma(wd, p.y, a.v);
     a.wsum += wd;
     a.sumAbs += fabs(wd);
 }
 
-// Separable base weights, all taps in range, support SUP (fully unrolled).
-template <int SUP>
+__device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float dy_ny, float dy_nx,
+                                    float wx, Acc &a) {
+    const float dx = dxf * c.rwF;
+    tapCore(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
+}
+
+// Separable base weights, all taps in range, support SUP: columns unrolled
+// with their products in registers, rows looped (keeps the loop body small
+// enough for the instruction cache). FULL: every tap active (no mask tests).
+template <int SUP, bool FULL>
 __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
                                               const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
-    float dxf[SUP], wxv[SUP];
+    float dx[SUP], wxv[SUP];
 #pragma unroll
     for (int i = 0; i < SUP; ++i) {
-        dxf[i] = (float)(tx0 + i) - c.scx;
+        dx[i] = ((float)(tx0 + i) - c.scx) * c.rwF;
         wxv[i] = __ldg(wxp + i);
     }
-#pragma unroll
-    for (int j = 0; j < SUP; ++j) {
-        if (!((my >> j) & 1u))
+    const float *lrow = c.lc + (size_t)ty0 * c.cw + tx0;
+    const double2 *uvrow = c.uv + (size_t)ty0 * c.cw + tx0;
+#pragma unroll 1
+    for (int j = 0; j < SUP; ++j, lrow += c.cw, uvrow += c.cw) {
+        if (!FULL && !((my >> j) & 1u))
             continue;
-        const size_t rowOff = (size_t)(ty0 + j) * c.cw + tx0;
         const float wy = __ldg(wyp + j);
         const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
         const float dy_ny = dy * c.ny, dy_nx = dy * c.nx;
 #pragma unroll
         for (int i = 0; i < SUP; ++i) {
-            if (!((mx >> i) & 1u))
+            if (!FULL && !((mx >> i) & 1u))
                 continue;
-            tap(c, rowOff + i, dxf[i], dy_ny, dy_nx, wxv[i] * wy, a);
+            tapCore(c, ldf(lrow + i), __ldg(uvrow + i), dx[i] * c.nx, -dx[i] * c.ny, dy_ny, dy_nx,
+                    wxv[i] * wy, a);
         }
     }
+}
+
+template <int SUP>
+__device__ __forceinline__ void tapsSeparableMasked(const TapCtx &c, int tx0, int ty0, const float *wxp,
+                                                    const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
+    const uint32_t full = (1u << SUP) - 1u;
+    if (mx == full && my == full)
+        tapsSeparable<SUP, true>(c, tx0, ty0, wxp, wyp, mx, my, a);
+    else
+        tapsSeparable<SUP, false>(c, tx0, ty0, wxp, wyp, mx, my, a);
 }
 
 // Any support, clamped taps; separable or radial base weights.
@@ -490,11 +603,11 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     Acc a{0.0, 0.0, 0.0, 0.0};
     const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup;
     if (fast && ax.sup == 8)
-        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
+        tapsSeparableMasked<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
     else if (fast && ax.sup == 6)
-        tapsSeparable<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
+        tapsSeparableMasked<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
     else if (fast && ax.sup == 4)
-        tapsSeparable<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
+        tapsSeparableMasked<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
     else
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
 

@@ -693,7 +693,7 @@ static void initShapes() {
 }
 
 bool stageTunable(int s) {
-    return s == S_PLAIN || s == S_HPASS || s == S_AFFINE || s == S_DET_TRANSFER || s == S_DET_PLAIN ||
+    return s == S_HPASS || s == S_AFFINE || s == S_DET_TRANSFER || s == S_DET_PLAIN ||
            s == S_LGF_DENSE || s == S_YC || s == S_BM_AGG;
 }
 
@@ -717,7 +717,7 @@ int guidedVariant() {
     std::lock_guard<std::mutex> lock(gShapeMu);
     if (gGuidedVariant < 0) {
         const char *e = std::getenv("LGCR_GUIDED_VARIANT");
-        gGuidedVariant = (e && e[0] == '1') ? 1 : 0;
+        gGuidedVariant = (e && e[0] == '0') ? 0 : 1;
     }
     return gGuidedVariant;
 }
@@ -736,7 +736,7 @@ static int stageTiles(const FrameJob &J, int s) {
         int bx, by;
         stageShape(s, bx, by);
         switch (s) {
-        case S_PLAIN: case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
+        case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
         case S_HPASS: return cdiv(J.W, bx) * cdiv(J.ch, by);
         case S_AFFINE: case S_LGF_DENSE: case S_YC: return cdiv(J.cw, bx) * cdiv(J.ch, by);
         case S_DET_PLAIN: return cdiv(J.sw, bx) * cdiv(J.sh, by);
@@ -765,7 +765,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_HPASS: return (J.hTab && !J.radial && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
-    case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, kPlainRows);
     case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC:
     case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
