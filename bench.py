@@ -124,7 +124,7 @@ class Clocks:
 def read_traffic():
     """Per-launch DRAM traffic of the dominant stage from the committed ncu
     summary (line 'traffic_bytes_per_output_pixel: X'), scaled by pixels."""
-    path = os.path.join(ROOT, "profiles", "reconstructChroma_batched_config.md")
+    path = os.path.join(ROOT, "profiles", "recon_kernels_batched_8frames.md")
     try:
         m = re.search(r"traffic_bytes_per_output_pixel:\s*([0-9.eE+-]+)", open(path).read())
         return float(m.group(1)) if m else None
