@@ -341,7 +341,9 @@ def our_arm(args):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s",
                               "frames_per_step": len(specs), "batch_only": True,
-                              "ms_per_step": round(max_ms / args.steps, 3)}))
+                              "ms_per_step": round(max_ms / args.steps, 3),
+                              "stage_ms_per_step": {k: round(v / max(1, args.steps), 3) for k, v in
+                                                    sorted(stage_ms.items(), key=lambda kv: -kv[1])}}))
         if world > 1:
             torch.distributed.destroy_process_group()
         return 0

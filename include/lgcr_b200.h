@@ -178,6 +178,14 @@ int lgcr_debug_axis(const lgcr_recon *filter, int axis, double shift, int *start
                     float *w, uint8_t *am, float *pos, float *lpos, int *chroma_i0,
                     float *chroma_f, int *luma_i0, float *luma_f, int *sup);
 
+/* Self-check of the device reciprocal the guided taps use for their
+ * 1/(1 + ...) similarity and bump terms (src/recon.cpp:615-619 divides):
+ * compares it with the IEEE quotient 1.0f/x for every float x in [1, 2^64)
+ * plus the special arguments, on the current device. Writes the number of
+ * differing results to *mismatches (0 expected). No counterpart in the
+ * reference (its divides are plain C++). */
+int lgcr_selftest_reciprocal(uint64_t *mismatches);
+
 /* ---------------------------------------------------------------------
  * Batched form: many frames (any mix of filters, sizes, subsamplings and
  * depths) in one launch per pipeline stage, captured as a CUDA graph and

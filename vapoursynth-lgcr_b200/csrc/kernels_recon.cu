@@ -291,9 +291,9 @@ __device__ __forceinline__ void tapCore(const TapCtx &c, float l, double2 p, flo
     const float dL = l - c.L0;
     const float dp = dxnx + dy_ny;
     const float dt = dxny + dy_nx;
-    const float simRaw = 1.0f / (1.0f + dL * dL * c.invSigma2);
+    const float simRaw = rcpAtLeastOne(1.0f + dL * dL * c.invSigma2);
     const float sim = 1.0f - c.guideFade * (1.0f - simRaw);
-    const float bump = 1.0f / (1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par);
+    const float bump = rcpAtLeastOne(1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par);
     const float w = sim * (wx + c.rescue * bump);
     const double wd = (double)w;
     a.u = fma(wd, p.x, a.u);
@@ -308,45 +308,35 @@ __device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float 
     tapCore(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
 }
 
-// Separable base weights, all taps in range, support SUP: columns unrolled
-// with their products in registers, rows looped (keeps the loop body small
-// enough for the instruction cache). FULL: every tap active (no mask tests).
-template <int SUP, bool FULL>
+// Separable base weights, all taps in range, support SUP (fully unrolled;
+// the per-column products dx*nx and (-dx)*ny stay in registers).
+template <int SUP>
 __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
                                               const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
-    float dx[SUP], wxv[SUP];
+    float dxnx[SUP], dxny[SUP], wxv[SUP];
 #pragma unroll
     for (int i = 0; i < SUP; ++i) {
-        dx[i] = ((float)(tx0 + i) - c.scx) * c.rwF;
+        const float dx = ((float)(tx0 + i) - c.scx) * c.rwF;
+        dxnx[i] = dx * c.nx;
+        dxny[i] = -dx * c.ny;
         wxv[i] = __ldg(wxp + i);
     }
-    const float *lrow = c.lc + (size_t)ty0 * c.cw + tx0;
-    const double2 *uvrow = c.uv + (size_t)ty0 * c.cw + tx0;
-#pragma unroll 1
-    for (int j = 0; j < SUP; ++j, lrow += c.cw, uvrow += c.cw) {
-        if (!FULL && !((my >> j) & 1u))
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((my >> j) & 1u))
             continue;
+        const float *lrow = c.lc + (size_t)(ty0 + j) * c.cw + tx0;
+        const double2 *uvrow = c.uv + (size_t)(ty0 + j) * c.cw + tx0;
         const float wy = __ldg(wyp + j);
         const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
         const float dy_ny = dy * c.ny, dy_nx = dy * c.nx;
 #pragma unroll
         for (int i = 0; i < SUP; ++i) {
-            if (!FULL && !((mx >> i) & 1u))
+            if (!((mx >> i) & 1u))
                 continue;
-            tapCore(c, ldf(lrow + i), __ldg(uvrow + i), dx[i] * c.nx, -dx[i] * c.ny, dy_ny, dy_nx,
-                    wxv[i] * wy, a);
+            tapCore(c, ldf(lrow + i), __ldg(uvrow + i), dxnx[i], dxny[i], dy_ny, dy_nx, wxv[i] * wy, a);
         }
     }
-}
-
-template <int SUP>
-__device__ __forceinline__ void tapsSeparableMasked(const TapCtx &c, int tx0, int ty0, const float *wxp,
-                                                    const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
-    const uint32_t full = (1u << SUP) - 1u;
-    if (mx == full && my == full)
-        tapsSeparable<SUP, true>(c, tx0, ty0, wxp, wyp, mx, my, a);
-    else
-        tapsSeparable<SUP, false>(c, tx0, ty0, wxp, wyp, mx, my, a);
 }
 
 // Any support, clamped taps; separable or radial base weights.
@@ -603,11 +593,11 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     Acc a{0.0, 0.0, 0.0, 0.0};
     const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup;
     if (fast && ax.sup == 8)
-        tapsSeparableMasked<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
+        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
     else if (fast && ax.sup == 6)
-        tapsSeparableMasked<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
+        tapsSeparable<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
     else if (fast && ax.sup == 4)
-        tapsSeparableMasked<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
+        tapsSeparable<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
     else
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
 

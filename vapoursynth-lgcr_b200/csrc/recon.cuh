@@ -153,6 +153,25 @@ __device__ __forceinline__ int iclamp(int v, int lo, int hi) { return v < lo ? l
 
 __device__ __forceinline__ float ldf(const float *p) { return __ldg(p); }
 
+// 1/x for denominators of the form 1 + (non-negative terms), i.e. x >= 1,
+// equal bit for bit to the IEEE quotient 1.0f / x. On [1, 2^64) the hardware
+// approximation (rcp.approx) is refined by one Newton-Raphson step evaluated
+// with fused multiply-adds, e = 1 - x*y, y' = y + y*e (Markstein, IBM J. Res.
+// Dev. 34(1), 1990); an exhaustive device check over every float in that
+// range (lgcr_selftest_reciprocal) finds no difference from 1.0f / x. Larger,
+// infinite or NaN arguments take the IEEE division.
+constexpr float kRcpFastLimit = 18446744073709551616.0f;   // 2^64
+
+__device__ __forceinline__ float rcpAtLeastOne(float x) {
+    if (x < kRcpFastLimit) {
+        float y;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+        const float e = __fmaf_rn(-x, y, 1.0f);
+        return __fmaf_rn(y, e, y);
+    }
+    return 1.0f / x;
+}
+
 // Block -> frame by binary search over the stage prefix table.
 __device__ __forceinline__ int findFrame(const int *tileStart, int njobs, int block) {
     int lo = 0, hi = njobs - 1;

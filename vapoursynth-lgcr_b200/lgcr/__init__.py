@@ -20,7 +20,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(HERE, "liblgcr_b200.so")
+# LGCR_B200_LIBRARY selects another build of the library (a different path)
+LIBPATH = os.environ.get("LGCR_B200_LIBRARY") or os.path.join(HERE, "liblgcr_b200.so")
 UNSET_INT = -(2 ** 31)
 
 LGCR_OK = 0
