@@ -14,9 +14,31 @@ namespace lgcr_b200 {
 constexpr int kPlainRows = 32;
 constexpr int kPlainStagedRows = 40;
 
+// k_convert: samples per warp (one row segment) and warps per block; the
+// luma blocks of a frame come first, then the chroma blocks.
+constexpr int kConvertSpan = 256;
+constexpr int kConvertWarps = 8;
+__host__ __device__ __forceinline__ int convertBlocks(int w, int h) {
+    return (h * ((w + kConvertSpan - 1) / kConvertSpan) + kConvertWarps - 1) / kConvertWarps;
+}
+__host__ __device__ __forceinline__ int convertLumaBlocks(int sw, int sh) { return convertBlocks(sw, sh); }
+
+// k_tensor: columns each warp emits, warps per block (side by side), rows
+// per strip.
+constexpr int kTensorCols = 28;
+constexpr int kTensorWarps = 8;
+constexpr int kTensorRows = 32;
+
+// k_dilate_h: widest row in mask words and the zero words on either side
+// (the dilation radius must stay below 32 * kDilPadWords).
+constexpr int kDilMaxWords = 2048;
+constexpr int kDilPadWords = 8;
+
+// k_count: chroma mask bytes per block.
+constexpr int kCountChunk = 16384;
+
 __global__ void k_convert(LGCR_STAGE_ARGS);
 __global__ void k_tensor(LGCR_STAGE_ARGS);
-__global__ void k_lc(LGCR_STAGE_ARGS);
 __global__ void k_dilate_h(LGCR_STAGE_ARGS);
 __global__ void k_dilate_v(LGCR_STAGE_ARGS);
 __global__ void k_mark_chroma(LGCR_STAGE_ARGS);

@@ -309,7 +309,7 @@ __device__ __forceinline__ bool activeOut(const FrameJob &J, int ox, int oy) {
         return true;
     const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
     const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
-    return J.mask[(size_t)my * J.sw + mx] != 0;
+    return maskAt(J, mx, my) != 0;
 }
 
 __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {

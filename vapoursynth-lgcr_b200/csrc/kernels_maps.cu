@@ -1,349 +1,430 @@
 // Map-building stages of the Recon path (all HBM-bound stencils):
-//   k_convert      planeToFloat                       src/lgcr.h:986-995
-//   k_tensor       sobelTensor3x3 + trust seed        src/maps.cpp:9-168
-//   k_lc           buildLcMap (scalar footprint sum)  src/maps.cpp:425-499
-//   k_dilate_h/v   buildTrustMask dilation            src/maps.cpp:280-340
-//   k_mark_chroma  buildSparseWorkset chroma mask     src/maps.cpp:342-422
-//   k_gate         buildMutualGate                    src/maps.cpp:831-948
+//   k_convert      planeToFloat                  src/lgcr.h:986-995
+//                  + buildLcMap footprint sums    src/maps.cpp:425-499
+//   k_tensor       sobelTensor3x3 + trust seed   src/maps.cpp:9-168
+//   k_dilate_h/v   buildTrustMask dilation       src/maps.cpp:280-340
+//   k_mark_chroma  buildSparseWorkset            src/maps.cpp:342-422
+//   k_count        active chroma samples         src/maps.cpp:398-420
+//   k_gate         buildMutualGate               src/maps.cpp:831-948
+//
+// The dilated trust mask is stored one bit per luma sample (rows of
+// maskWords 32-bit words, bit i of word k = column 32k + i): the dilation
+// runs on whole words and later stages test single bits.
 #include "kernels.cuh"
 
 namespace lgcr_b200 {
 
 // ---------------------------------------------------------------------------
-// input conversion: one thread per luma pixel (also converts the chroma
-// sample at the same coordinates when it exists) and, for same-size output,
-// copies the luma code to the output plane (the shared luma plane).
+// Input conversion with the footprint luma map folded in. A warp converts
+// kConvertSpan consecutive samples of one row, lane l taking samples l,
+// l + 32, ... so every load and store is one coalesced row segment. The
+// first convertLumaBlocks(J) blocks of a frame cover the luma plane (and copy
+// it to a same-size output), the rest the chroma planes; the chroma blocks
+// also clear the chroma work masks and compute lc from the luma codes.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float loadSample(const FrameJob &J, int plane, int x, int y) {
-    const char *row = static_cast<const char *>(J.in[plane]) + (long long)y * J.inPitch[plane];
-    if (J.inKind == kF32)
-        return reinterpret_cast<const float *>(row)[x];
-    const double s = (J.inKind == kU8) ? (double)reinterpret_cast<const uint8_t *>(row)[x]
-                                       : (double)reinterpret_cast<const uint16_t *>(row)[x];
-    const double off = plane == 0 ? 0.0 : J.cOffset;
-    return (float)(s * J.yScale + off);
+__device__ __forceinline__ uint32_t rawAt(const void *plane, long long pitch, int kind, int x, int y) {
+    const char *row = static_cast<const char *>(plane) + (long long)y * pitch;
+    if (kind == kU16)
+        return __ldg(reinterpret_cast<const unsigned short *>(row) + x);
+    if (kind == kU8)
+        return __ldg(reinterpret_cast<const unsigned char *>(row) + x);
+    return __float_as_uint(__ldg(reinterpret_cast<const float *>(row) + x));
 }
 
-__global__ void k_convert(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart,
-                          int njobs) {
+// planeToFloat of one sample: s * scale + offset in double, then float.
+__device__ __forceinline__ float toFloat(const FrameJob &J, uint32_t raw, double off) {
+    return J.inKind == kF32 ? __uint_as_float(raw) : (float)((double)raw * J.yScale + off);
+}
+
+__device__ __forceinline__ void storeRaw(void *plane, long long pitch, int kind, int x, int y, uint32_t raw) {
+    char *row = static_cast<char *>(plane) + (long long)y * pitch;
+    if (kind == kU16) reinterpret_cast<unsigned short *>(row)[x] = (unsigned short)raw;
+    else if (kind == kU8) reinterpret_cast<unsigned char *>(row)[x] = (unsigned char)raw;
+    else reinterpret_cast<uint32_t *>(row)[x] = raw;
+}
+
+__global__ void __launch_bounds__(kConvertWarps * 32)
+k_convert(LGCR_STAGE_ARGS) {
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
-    const int tilesX = (J.sw + 31) / 32;
-    const int x = (tile % tilesX) * 32 + threadIdx.x;
-    const int y = (tile / tilesX) * 8 + threadIdx.y;
-    if (x >= J.sw || y >= J.sh)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lumaBlocks = convertLumaBlocks(J.sw, J.sh);
+    if (tile < lumaBlocks) {
+        const int gpr = (J.sw + kConvertSpan - 1) / kConvertSpan;
+        const int gw = tile * kConvertWarps + warp;
+        if (gw >= J.sh * gpr)
+            return;
+        if (gw == 0 && lane < kCntCount)
+            J.counters[lane] = 0ull;
+        const int y = gw / gpr, xb = (gw % gpr) * kConvertSpan;
+        const bool copy = J.writeLuma && J.sameSize;
+#pragma unroll 4
+        for (int k = 0; k < kConvertSpan / 32; ++k) {
+            const int x = xb + lane + 32 * k;
+            if (x >= J.sw)
+                break;
+            const uint32_t raw = rawAt(J.in[0], J.inPitch[0], J.inKind, x, y);
+            if (J.Yw)
+                J.Yw[(size_t)y * J.sw + x] = toFloat(J, raw, 0.0);
+            if (copy)
+                storeRaw(J.out[0], J.outPitch[0], J.inKind, x, y, raw);
+        }
         return;
-    if (x == 0 && y == 0)
-        for (int k = 0; k < kCntCount; ++k)
-            J.counters[k] = 0ull;
-    if (J.Yw)
-        J.Yw[(size_t)y * J.sw + x] = loadSample(J, 0, x, y);
-    if (J.writeLuma && J.sameSize) {
-        const char *src = static_cast<const char *>(J.in[0]) + (long long)y * J.inPitch[0];
-        char *dst = static_cast<char *>(J.out[0]) + (long long)y * J.outPitch[0];
-        if (J.inKind == kU8) reinterpret_cast<uint8_t *>(dst)[x] = reinterpret_cast<const uint8_t *>(src)[x];
-        else if (J.inKind == kU16) reinterpret_cast<uint16_t *>(dst)[x] = reinterpret_cast<const uint16_t *>(src)[x];
-        else reinterpret_cast<float *>(dst)[x] = reinterpret_cast<const float *>(src)[x];
     }
-    if (x < J.cw && y < J.ch) {
-        const size_t o = (size_t)y * J.cw + x;
-        if (J.cmask) J.cmask[o] = 0;
-        if (J.roi) J.roi[o] = 0;
-        const float u = loadSample(J, 1, x, y), v = loadSample(J, 2, x, y);
+    const int gpr = (J.cw + kConvertSpan - 1) / kConvertSpan;
+    const int gw = (tile - lumaBlocks) * kConvertWarps + warp;
+    if (gw >= J.ch * gpr)
+        return;
+    const int cy = gw / gpr, xb = (gw % gpr) * kConvertSpan;
+    int yb = 0, ye = 0;
+    if (J.lc) {
+        yb = __ldg(J.lcYb + cy);
+        ye = __ldg(J.lcYe + cy);
+    }
+#pragma unroll 2
+    for (int k = 0; k < kConvertSpan / 32; ++k) {
+        const int cx = xb + lane + 32 * k;
+        if (cx >= J.cw)
+            break;
+        const size_t o = (size_t)cy * J.cw + cx;
+        const float u = toFloat(J, rawAt(J.in[1], J.inPitch[1], J.inKind, cx, cy), J.cOffset);
+        const float v = toFloat(J, rawAt(J.in[2], J.inPitch[2], J.inKind, cx, cy), J.cOffset);
         if (J.Uw) J.Uw[o] = u;
         if (J.Vw) J.Vw[o] = v;
         if (J.uvd) reinterpret_cast<double2 *>(J.uvd)[o] = make_double2((double)u, (double)v);
+        if (J.cmask) J.cmask[o] = 0;
+        if (J.roi) J.roi[o] = 0;
+        if (J.lc) {
+            // buildLcMap: raster-order double sum over the footprint
+            const int xb0 = __ldg(J.lcXb + cx), xe0 = __ldg(J.lcXe + cx);
+            double sum = 0.0;
+            for (int j = yb; j < ye; ++j)
+                for (int i = xb0; i < xe0; ++i)
+                    sum += (double)toFloat(J, rawAt(J.in[0], J.inPitch[0], J.inKind, i, j), 0.0);
+            J.lc[o] = (float)(sum / ((double)(xe0 - xb0) * (double)(ye - yb)));
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Structure tensor: Sobel/8 gradients (clamped), vertical 3-row sums of the
-// outer products, horizontal 3-tap box with the reference's border rule
-// ((2a+b)/9 and (a+2b)/9 at the ends, *(1/9) inside), trust seed
-// jxx + jyy > thr.  Tile TX x TY with a 2-pixel clamped halo in shared.
+// Structure tensor: Sobel/8 gradients at clamped positions, vertical 3-row
+// sums of the outer products, horizontal 3-tap box with the reference's
+// border rule ((2a+b)/9 and (a+2b)/9 at the ends, *(1/9) inside), trust
+// seed jxx + jyy > thr.
+//
+// Each warp walks down a strip of kTensorRows rows over 32 consecutive
+// columns x0-2 .. x0+29 and emits the 28 middle ones: lane values are luma
+// samples at clamped columns, horizontal neighbours come from shuffles, the
+// three gradient rows and their products roll in registers. The warps of a
+// block sit side by side.
 // ---------------------------------------------------------------------------
-constexpr int TT_X = 32, TT_Y = 16;
+struct Tri { float l, m, r; };
 
-__global__ void __launch_bounds__(TT_X * 8)
-k_tensor(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    __shared__ float ys[TT_Y + 4][TT_X + 4];
-    __shared__ float gxs[TT_Y + 2][TT_X + 2];
-    __shared__ float gys[TT_Y + 2][TT_X + 2];
-    __shared__ float vxx[TT_Y][TT_X + 2], vxy[TT_Y][TT_X + 2], vyy[TT_Y][TT_X + 2];
+__device__ __forceinline__ Tri tri(float v) {
+    return { __shfl_up_sync(0xffffffffu, v, 1), v, __shfl_down_sync(0xffffffffu, v, 1) };
+}
+
+// t = row above, c = centre row, b = row below (maps.cpp Sobel/8 order)
+__device__ __forceinline__ void sobel(const Tri &t, const Tri &c, const Tri &b, float &gx, float &gy) {
+    gx = (t.r + 2.0f * c.r + b.r - t.l - 2.0f * c.l - b.l) * 0.125f;
+    gy = (b.l + 2.0f * b.m + b.r - t.l - 2.0f * t.m - t.r) * 0.125f;
+}
+
+__global__ void __launch_bounds__(kTensorWarps * 32)
+k_tensor(LGCR_STAGE_ARGS) {
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
     const int w = J.sw, h = J.sh;
-    const int tilesX = (w + TT_X - 1) / TT_X;
-    const int x0 = (tile % tilesX) * TT_X, y0 = (tile / tilesX) * TT_Y;
-    const int tid = threadIdx.y * TT_X + threadIdx.x;
-    const int nthreads = TT_X * 8;
-    const float *Y = J.Y;
-    for (int i = tid; i < (TT_Y + 4) * (TT_X + 4); i += nthreads) {
-        const int r = i / (TT_X + 4), c = i % (TT_X + 4);
-        const int gy = iclamp(y0 - 2 + r, 0, h - 1), gx = iclamp(x0 - 2 + c, 0, w - 1);
-        ys[r][c] = ldf(Y + (size_t)gy * w + gx);
+    constexpr int span = kTensorCols * kTensorWarps;
+    const int tilesX = (w + span - 1) / span;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x0 = (tile % tilesX) * span + warp * kTensorCols;
+    if (x0 >= w)
+        return;                                   // whole warp
+    const int y0 = (tile / tilesX) * kTensorRows;
+    const int y1 = min(y0 + kTensorRows, h);
+    const int c = x0 - 2 + lane;
+    const bool emitLane = lane >= 2 && lane < 2 + kTensorCols && c < w;
+    const float *col = J.Y + iclamp(c, 0, w - 1);
+    auto L = [&](int r) { return ldf(col + (size_t)iclamp(r, 0, h - 1) * w); };
+
+    // G(r) = gradient at row clamp(r); prologue G(y0-1), G(y0)
+    const Tri la = tri(L(y0 - 2)), lb = tri(L(y0 - 1));
+    Tri rm = tri(L(y0)), rn = tri(L(y0 + 1));
+    float gxA, gyA, gxB, gyB;
+    sobel(lb, rm, rn, gxB, gyB);
+    if (y0 == 0) {
+        gxA = gxB;
+        gyA = gyB;
+    } else {
+        sobel(la, lb, rm, gxA, gyA);
     }
-    __syncthreads();
-    // gradients at clamped positions of rows y0-1..y0+TY, cols x0-1..x0+TX
-    for (int i = tid; i < (TT_Y + 2) * (TT_X + 2); i += nthreads) {
-        const int r = i / (TT_X + 2), c = i % (TT_X + 2);
-        const int gy = iclamp(y0 - 1 + r, 0, h - 1), gx = iclamp(x0 - 1 + c, 0, w - 1);
-        const int sr = gy - y0 + 2, sc = gx - x0 + 2;
-        const float tl = ys[sr - 1][sc - 1], t = ys[sr - 1][sc], tr = ys[sr - 1][sc + 1];
-        const float l = ys[sr][sc - 1], rr = ys[sr][sc + 1];
-        const float bl = ys[sr + 1][sc - 1], b = ys[sr + 1][sc], br = ys[sr + 1][sc + 1];
-        gxs[r][c] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
-        gys[r][c] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
-    }
-    __syncthreads();
-    // vertical sums for rows y0..y0+TY-1 at cols x0-1..x0+TX
-    for (int i = tid; i < TT_Y * (TT_X + 2); i += nthreads) {
-        const int r = i / (TT_X + 2), c = i % (TT_X + 2);
-        const float ax0 = gxs[r][c], ax1 = gxs[r + 1][c], ax2 = gxs[r + 2][c];
-        const float ay0 = gys[r][c], ay1 = gys[r + 1][c], ay2 = gys[r + 2][c];
-        vxx[r][c] = ax0 * ax0 + ax1 * ax1 + ax2 * ax2;
-        vxy[r][c] = ax0 * ay0 + ax1 * ay1 + ax2 * ay2;
-        vyy[r][c] = ay0 * ay0 + ay1 * ay1 + ay2 * ay2;
-    }
-    __syncthreads();
+    float pxxA = gxA * gxA, pxyA = gxA * gyA, pyyA = gyA * gyA;
+    float pxxB = gxB * gxB, pxyB = gxB * gyB, pyyB = gyB * gyB;
     const float ninth = 1.0f / 9.0f;
-    for (int i = tid; i < TT_Y * TT_X; i += nthreads) {
-        const int r = i / TT_X, c = i % TT_X;
-        const int x = x0 + c, y = y0 + r;
-        if (x >= w || y >= h)
-            continue;
-        const int cc = c + 1;
-        float oxx, oxy, oyy;
-        if (x == 0) {
-            const int rc = (w > 1) ? cc + 1 : cc;
-            oxx = (2.0f * vxx[r][cc] + vxx[r][rc]) / 9.0f;
-            oxy = (2.0f * vxy[r][cc] + vxy[r][rc]) / 9.0f;
-            oyy = (2.0f * vyy[r][cc] + vyy[r][rc]) / 9.0f;
-        } else if (x == w - 1) {
-            oxx = (vxx[r][cc - 1] + 2.0f * vxx[r][cc]) / 9.0f;
-            oxy = (vxy[r][cc - 1] + 2.0f * vxy[r][cc]) / 9.0f;
-            oyy = (vyy[r][cc - 1] + 2.0f * vyy[r][cc]) / 9.0f;
+    const float thr = J.trustThr;
+    float pf = L(y0 + 2);
+    for (int y = y0; y < y1; ++y) {
+        const Tri re = tri(pf);                   // luma row clamp(y + 2)
+        pf = L(y + 3);
+        float gxC, gyC;
+        if (y + 1 < h) {
+            sobel(rm, rn, re, gxC, gyC);
         } else {
-            oxx = ninth * (vxx[r][cc - 1] + vxx[r][cc] + vxx[r][cc + 1]);
-            oxy = ninth * (vxy[r][cc - 1] + vxy[r][cc] + vxy[r][cc + 1]);
-            oyy = ninth * (vyy[r][cc - 1] + vyy[r][cc] + vyy[r][cc + 1]);
+            gxC = gxB;
+            gyC = gyB;
         }
-        const size_t o = (size_t)y * w + x;
-        J.jxx[o] = oxx;
-        J.jxy[o] = oxy;
-        J.jyy[o] = oyy;
-        if (J.trustOn)
-            J.seed[o] = (oxx + oyy > J.trustThr) ? 1 : 0;
+        const float pxxC = gxC * gxC, pxyC = gxC * gyC, pyyC = gyC * gyC;
+        const float vxx = pxxA + pxxB + pxxC;
+        const float vxy = pxyA + pxyB + pxyC;
+        const float vyy = pyyA + pyyB + pyyC;
+        const float lxx = __shfl_up_sync(0xffffffffu, vxx, 1), rxx = __shfl_down_sync(0xffffffffu, vxx, 1);
+        const float lxy = __shfl_up_sync(0xffffffffu, vxy, 1), rxy = __shfl_down_sync(0xffffffffu, vxy, 1);
+        const float lyy = __shfl_up_sync(0xffffffffu, vyy, 1), ryy = __shfl_down_sync(0xffffffffu, vyy, 1);
+        if (emitLane) {
+            float oxx, oxy, oyy;
+            if (c == 0) {
+                const bool wide = w > 1;
+                oxx = (2.0f * vxx + (wide ? rxx : vxx)) / 9.0f;
+                oxy = (2.0f * vxy + (wide ? rxy : vxy)) / 9.0f;
+                oyy = (2.0f * vyy + (wide ? ryy : vyy)) / 9.0f;
+            } else if (c == w - 1) {
+                oxx = (lxx + 2.0f * vxx) / 9.0f;
+                oxy = (lxy + 2.0f * vxy) / 9.0f;
+                oyy = (lyy + 2.0f * vyy) / 9.0f;
+            } else {
+                oxx = ninth * (lxx + vxx + rxx);
+                oxy = ninth * (lxy + vxy + rxy);
+                oyy = ninth * (lyy + vyy + ryy);
+            }
+            const size_t o = (size_t)y * w + c;
+            J.jxx[o] = oxx;
+            J.jxy[o] = oxy;
+            J.jyy[o] = oyy;
+            if (J.trustOn)
+                J.seed[o] = (oxx + oyy > thr) ? 1 : 0;
+        }
+        pxxA = pxxB; pxyA = pxyB; pyyA = pyyB;
+        pxxB = pxxC; pxyB = pxyC; pyyB = pyyC;
+        gxB = gxC; gyB = gyC;
+        rm = rn;
+        rn = re;
     }
 }
 
 // ---------------------------------------------------------------------------
-// Footprint luma per chroma sample: double sum in raster order.
+// Trust-mask dilation: square window of radius r clipped to the plane (the
+// reference's rolling population counts give the same set).
+// Horizontal: one block per row packs the seed bytes into words in shared
+// memory and ORs the word stream shifted by 1..r either way (funnel shifts
+// across word boundaries). Needs r <= 32 * (kDilPadWords - 1).
 // ---------------------------------------------------------------------------
-__global__ void k_lc(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart,
-                     int njobs) {
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
-    const int tile = blockIdx.x - tileStart[f];
-    const int tilesX = (J.cw + 31) / 32;
-    const int cx = (tile % tilesX) * 32 + threadIdx.x;
-    const int cy = (tile / tilesX) * 8 + threadIdx.y;
-    if (cx >= J.cw || cy >= J.ch)
-        return;
-    const int xb = __ldg(J.lcXb + cx), xe = __ldg(J.lcXe + cx);
-    const int yb = __ldg(J.lcYb + cy), ye = __ldg(J.lcYe + cy);
-    double sum = 0.0;
-    for (int j = yb; j < ye; ++j) {
-        const float *row = J.Y + (size_t)j * J.sw;
-        for (int i = xb; i < xe; ++i)
-            sum += (double)ldf(row + i);
-    }
-    J.lc[(size_t)cy * J.cw + cx] = (float)(sum / ((double)(xe - xb) * (double)(ye - yb)));
+__device__ __forceinline__ uint32_t packNibble(uint32_t fourBytes) {
+    // bytes are 0 or 1: the product gathers byte i at bit 21 + i
+    return ((fourBytes * 0x204081u) >> 21) & 0xFu;
 }
 
-// ---------------------------------------------------------------------------
-// Trust-mask dilation: square window of radius r (rolling population count in
-// the reference; any-set in [x-r, x+r] here, same set).
-// Horizontal: one block per (1024-pixel segment, row) with a shared prefix.
-// ---------------------------------------------------------------------------
-constexpr int DIL_SEG = 1024;
-constexpr int DIL_MAXR = 512;
-
-__global__ void __launch_bounds__(256)
-k_dilate_h(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    __shared__ int pre[DIL_SEG + 2 * DIL_MAXR + 1];
-    __shared__ int warpTot[8];
+__global__ void __launch_bounds__(128)
+k_dilate_h(LGCR_STAGE_ARGS) {
+    __shared__ uint32_t words[kDilMaxWords + 2 * kDilPadWords];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
-    const int tile = blockIdx.x - tileStart[f];
-    const int w = J.sw;
-    const int segs = (w + DIL_SEG - 1) / DIL_SEG;
-    const int y = tile / segs;
-    const int x0 = (tile % segs) * DIL_SEG;
-    const int r = J.dil;
-    const int lo = x0 - r;
-    const int span = DIL_SEG + 2 * r;         // prefix over [lo, lo+span)
+    const int y = blockIdx.x - tileStart[f];
+    const int w = J.sw, mw = J.maskWords, r = J.dil;
     const uint8_t *src = J.seed + (size_t)y * w;
-    // chunked block scan
-    int carry = 0;
-    for (int base = 0; base < span; base += 256) {
-        const int i = base + threadIdx.x;
-        const int gx = lo + i;
-        int v = (i < span && gx >= 0 && gx < w) ? (src[gx] != 0) : 0;
-        // warp inclusive scan
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int n = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += n;
+    for (int k = threadIdx.x; k < mw + 2 * kDilPadWords; k += blockDim.x) {
+        const int wk = k - kDilPadWords;
+        uint32_t bits = 0;
+        if (wk >= 0 && wk < mw) {
+            const int x = wk * 32;
+            const uint8_t *p = src + x;
+            if (x + 32 <= w && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                const uint4 a = __ldg(reinterpret_cast<const uint4 *>(p));
+                const uint4 b = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+                bits = packNibble(a.x) | packNibble(a.y) << 4 | packNibble(a.z) << 8 |
+                       packNibble(a.w) << 12 | packNibble(b.x) << 16 | packNibble(b.y) << 20 |
+                       packNibble(b.z) << 24 | packNibble(b.w) << 28;
+            } else {
+                const int n = min(32, w - x);
+                for (int i = 0; i < n; ++i)
+                    bits |= (p[i] != 0 ? 1u : 0u) << i;
+            }
         }
-        if (lane == 31) warpTot[wid] = v;
-        __syncthreads();
-        int add = carry;
-        for (int k = 0; k < wid; ++k) add += warpTot[k];
-        if (i < span) pre[i + 1] = v + add;
-        int total = 0;
-        for (int k = 0; k < 8; ++k) total += warpTot[k];
-        __syncthreads();
-        carry += total;
+        words[k] = bits;
     }
-    if (threadIdx.x == 0) pre[0] = 0;
     __syncthreads();
-    uint8_t *dst = J.mtmp + (size_t)y * w;
-    for (int c = threadIdx.x; c < DIL_SEG; c += 256) {
-        const int x = x0 + c;
-        if (x >= w)
-            break;
-        // window [x-r, x+r] -> prefix indices [c, c+2r+1)
-        dst[x] = (pre[c + 2 * r + 1] - pre[c]) != 0;
-    }
-}
-
-// Vertical: 32 columns x DV_ROWS rows per block, rolling count per column
-// over the tile rows (plus halo) staged in shared memory.
-constexpr int DV_ROWS = 128;
-
-__global__ void __launch_bounds__(32)
-k_dilate_v(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    extern __shared__ uint8_t col[];   // (DV_ROWS + 2r) x 32
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
-    const int tile = blockIdx.x - tileStart[f];
-    const int w = J.sw, h = J.sh, r = J.dil;
-    const int tilesX = (w + 31) / 32;
-    const int x = (tile % tilesX) * 32 + threadIdx.x;
-    const int y0 = (tile / tilesX) * DV_ROWS;
-    const int rows = DV_ROWS + 2 * r;
-    for (int i = 0; i < rows; ++i) {
-        const int gy = y0 - r + i;
-        col[i * 32 + threadIdx.x] = (x < w && gy >= 0 && gy < h) ? J.mtmp[(size_t)gy * w + x] : 0;
-    }
-    __syncwarp();
-    if (x >= w)
-        return;
-    int count = 0;
-    for (int i = 0; i < 2 * r; ++i)
-        count += col[i * 32 + threadIdx.x] != 0;
-    for (int yy = 0; yy < DV_ROWS; ++yy) {
-        const int y = y0 + yy;
-        if (y >= h)
-            break;
-        count += col[(yy + 2 * r) * 32 + threadIdx.x] != 0;    // window [y-r, y+r]
-        J.mask[(size_t)y * w + x] = count != 0;
-        count -= col[yy * 32 + threadIdx.x] != 0;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Sparse workset: an output pixel is active when the mask sample its
-// position maps to is set; active pixels mark the 2x2 chroma bilinear
-// footprint. Counts active output pixels.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool outputActive(const FrameJob &J, int ox, int oy) {
-    const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
-    const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
-    return J.mask[(size_t)my * J.sw + mx] != 0;
-}
-
-__global__ void k_mark_chroma(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart,
-                              int njobs) {
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
-    const int tile = blockIdx.x - tileStart[f];
-    const int tilesX = (J.W + 31) / 32;
-    const int ox = (tile % tilesX) * 32 + threadIdx.x;
-    const int oy = (tile / tilesX) * 8 + threadIdx.y;
-    bool active = false;
-    if (ox < J.W && oy < J.H) {
-        active = J.sparse ? outputActive(J, ox, oy) : true;
-        if (active && J.sparse) {
-            const int cx0 = __ldg(J.ax.cbI0 + ox);
-            const int cx1 = min(cx0 + 1, J.cw - 1);
-            const int cy0 = __ldg(J.ay.cbI0 + oy);
-            const int cy1 = min(cy0 + 1, J.ch - 1);
-            uint8_t *m = J.cmask;
-            m[(size_t)cy0 * J.cw + cx0] = 1;
-            m[(size_t)cy0 * J.cw + cx1] = 1;
-            m[(size_t)cy1 * J.cw + cx0] = 1;
-            m[(size_t)cy1 * J.cw + cx1] = 1;
+    const int qmax = r >> 5;
+    for (int k = threadIdx.x; k < mw; k += blockDim.x) {
+        const uint32_t *W = words + kDilPadWords + k;
+        uint32_t acc = W[0];
+        for (int q = 0; q <= qmax; ++q) {
+            const uint32_t r0 = W[q], r1 = W[q + 1], l0 = W[-q], l1 = W[-q - 1];
+            if (q > 0)
+                acc |= r0 | l0;
+            const int smax = min(31, r - 32 * q);
+            for (int s = 1; s <= smax; ++s)
+                acc |= __funnelshift_r(r0, r1, s) | __funnelshift_l(l1, l0, s);
         }
+        if (k == mw - 1 && (w & 31))
+            acc &= (1u << (w & 31)) - 1u;
+        J.mtmp[(size_t)y * mw + k] = acc;
     }
-    // block-aggregated append to the frame's guided work list: one atomic
-    // per block (8 warps), warp offsets from a shared prefix
-    __shared__ unsigned warpCount[8];
-    __shared__ unsigned long long blockBase;
-    const unsigned ballot = __ballot_sync(0xffffffffu, active);
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    if (lane == 0)
-        warpCount[warp] = __popc(ballot);
+}
+
+// Vertical: one thread per mask word, OR over rows y-r .. y+r (clipped).
+// Also counts the set mask samples (one atomic per block).
+__global__ void __launch_bounds__(256)
+k_dilate_v(LGCR_STAGE_ARGS) {
+    __shared__ unsigned warpSum[8];
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    const int tile = blockIdx.x - tileStart[f];
+    const int mw = J.maskWords, h = J.sh, r = J.dil;
+    const int tilesX = (mw + 31) / 32;
+    const int k = (tile % tilesX) * 32 + threadIdx.x;
+    const int y = (tile / tilesX) * 8 + threadIdx.y;
+    unsigned count = 0;
+    if (k < mw && y < h) {
+        const int lo = max(0, y - r), hi = min(h - 1, y + r);
+        const uint32_t *col = J.mtmp + k;
+        uint32_t acc = 0;
+        for (int j = lo; j <= hi; ++j)
+            acc |= __ldg(col + (size_t)j * mw);
+        J.mask[(size_t)y * mw + k] = acc;
+        count = __popc(acc);
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        count += __shfl_down_sync(0xffffffffu, count, o);
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if ((tid & 31) == 0)
+        warpSum[tid >> 5] = count;
     __syncthreads();
     if (tid == 0) {
         unsigned total = 0;
-        for (int w = 0; w < 8; ++w) {
-            const unsigned c = warpCount[w];
-            warpCount[w] = total;
+        for (int i = 0; i < 8; ++i)
+            total += warpSum[i];
+        if (total)
+            atomicAdd(J.counters + kCntMaskPixels, (unsigned long long)total);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse workset: one thread per 32 output pixels of a row. An output pixel
+// is active when the mask sample its position maps to is set (every pixel
+// when the frame is not sparse); active pixels mark the 2x2 chroma bilinear
+// footprint. The block counts its active pixels, takes one range of the
+// frame's guided work list with one atomic, and each thread appends its
+// pixels (y << 16 | x) in column order at its prefix offset.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t activeWord(const FrameJob &J, int kw, int oy) {
+    const int x0 = kw * 32;
+    const int n = min(32, J.W - x0);
+    const uint32_t valid = n == 32 ? 0xffffffffu : ((1u << n) - 1u);
+    if (!J.sparse)
+        return valid;
+    if (J.sameSize)
+        return __ldg(J.mask + (size_t)oy * J.maskWords + kw) & valid;
+    const int my = min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
+    uint32_t bits = 0;
+    for (int i = 0; i < n; ++i) {
+        const int mx = min(J.sw - 1, (int)((long long)(x0 + i) * J.sw / J.W));
+        bits |= maskAt(J, mx, my) << i;
+    }
+    return bits;
+}
+
+__global__ void __launch_bounds__(256)
+k_mark_chroma(LGCR_STAGE_ARGS) {
+    __shared__ unsigned warpCount[8];
+    __shared__ unsigned long long blockBase;
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    const int tile = blockIdx.x - tileStart[f];
+    const int ow = (J.W + 31) / 32;
+    const int idx = tile * 256 + threadIdx.x;
+    const int oy = idx / ow, kw = idx % ow;
+    uint32_t bits = 0;
+    if (oy < J.H) {
+        bits = activeWord(J, kw, oy);
+        if (bits && J.sparse) {
+            const int cy0 = __ldg(J.ay.cbI0 + oy);
+            const int cy1 = min(cy0 + 1, J.ch - 1);
+            uint8_t *row0 = J.cmask + (size_t)cy0 * J.cw;
+            uint8_t *row1 = J.cmask + (size_t)cy1 * J.cw;
+            int written = -1;
+            for (uint32_t m = bits; m; m &= m - 1) {
+                const int ox = kw * 32 + __ffs(m) - 1;
+                const int cx0 = __ldg(J.ax.cbI0 + ox);
+                const int cx1 = min(cx0 + 1, J.cw - 1);
+                if (cx0 > written) { row0[cx0] = 1; row1[cx0] = 1; }
+                if (cx1 > written) { row0[cx1] = 1; row1[cx1] = 1; }
+                written = max(written, cx1);
+            }
+        }
+    }
+    // block prefix of the active counts
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned cnt = __popc(bits);
+    unsigned incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned n = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += n;
+    }
+    if (lane == 31)
+        warpCount[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned total = 0;
+        for (int i = 0; i < 8; ++i) {
+            const unsigned c = warpCount[i];
+            warpCount[i] = total;
             total += c;
         }
         blockBase = total ? atomicAdd(J.counters + kCntActiveOutput, (unsigned long long)total) : 0ull;
     }
     __syncthreads();
-    if (active && J.listed) {
-        const unsigned rank = warpCount[warp] + __popc(ballot & ((1u << lane) - 1u));
-        J.actList[blockBase + rank] = ((uint32_t)oy << 16) | (uint32_t)ox;
+    if (bits && J.listed) {
+        unsigned long long pos = blockBase + warpCount[warp] + incl - cnt;
+        const uint32_t rowCode = (uint32_t)oy << 16;
+        for (uint32_t m = bits; m; m &= m - 1)
+            J.actList[pos++] = rowCode | (uint32_t)(kw * 32 + __ffs(m) - 1);
     }
 }
 
-// Population count of a u8 plane region: counts chroma mask / trust mask.
-__global__ void k_count(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart,
-                        int njobs) {
+// Active chroma samples: population count of the 0/1 chroma mask bytes,
+// 16 bytes per thread per step, one atomic per block.
+__global__ void __launch_bounds__(256)
+k_count(LGCR_STAGE_ARGS) {
+    __shared__ unsigned warpSum[8];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
     const size_t nc = (size_t)J.cw * J.ch;
-    const size_t nm = (size_t)J.sw * J.sh;
-    const size_t i = (size_t)tile * 1024 + threadIdx.x * 4;
-    int c = 0, m = 0;
-    for (int k = 0; k < 4; ++k) {
-        if (i + k < nc) c += J.cmask[i + k] != 0;
-        if (i + k < nm) m += J.mask[i + k] != 0;
+    const size_t base = (size_t)tile * kCountChunk;
+    const size_t end = min(nc, base + kCountChunk);
+    unsigned c = 0;
+    for (size_t i = base + threadIdx.x * 16; i < end; i += 256 * 16) {
+        if (i + 16 <= end) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(J.cmask + i));
+            c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+        } else {
+            for (size_t k = i; k < end; ++k)
+                c += J.cmask[k] != 0;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 16; o > 0; o >>= 1)
         c += __shfl_down_sync(0xffffffffu, c, o);
-        m += __shfl_down_sync(0xffffffffu, m, o);
-    }
-    __shared__ int sc[8], sm[8];
-    if ((threadIdx.x & 31) == 0) {
-        sc[threadIdx.x >> 5] = c;
-        sm[threadIdx.x >> 5] = m;
-    }
+    if ((threadIdx.x & 31) == 0)
+        warpSum[threadIdx.x >> 5] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int tc = 0, tm = 0;
-        for (int w = 0; w < 8; ++w) { tc += sc[w]; tm += sm[w]; }
-        if (tc) atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)tc);
-        if (tm) atomicAdd(J.counters + kCntMaskPixels, (unsigned long long)tm);
+        unsigned total = 0;
+        for (int i = 0; i < 8; ++i)
+            total += warpSum[i];
+        if (total)
+            atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)total);
     }
 }
 

@@ -139,7 +139,7 @@ __device__ __forceinline__ bool pixelActive(const FrameJob &J, int ox, int oy) {
         return true;
     const int mx = J.sameSize ? ox : min(J.sw - 1, (int)((long long)ox * J.sw / J.W));
     const int my = J.sameSize ? oy : min(J.sh - 1, (int)((long long)oy * J.sh / J.H));
-    return J.mask[(size_t)my * J.sw + mx] != 0;
+    return maskAt(J, mx, my) != 0;
 }
 
 // Final sample of one output pixel: to the typed output plane when this

@@ -159,6 +159,13 @@ int createFilter(const lgcr_params *pp, const lgcr_format *fmt, Filter **out, st
         return fail("LGCR: invalid parameter range (need 0<=strength/rescue<=1, 0<=bp/ms/qgate<=1, "
                     "sigma/sratio/sdb/gsigma/reg>0, stretch>=0)");
 
+    // device-path limits (no reference counterpart): work lists pack output
+    // coordinates into 16 bits, mask rows span at most kDilMaxWords words
+    if (fmt->width > 65535 || fmt->height > 65535 || d.outW > 65535 || d.outH > 65535)
+        return fail("LGCR: frame dimensions above 65535 are not supported on the device path");
+    if (int(std::ceil(ks.support * 2.0)) + 8 >= 32 * kDilPadWords)
+        return fail("LGCR: kernel support too large for the trust-mask dilation");
+
     f->sw = fmt->width;
     f->sh = fmt->height;
     f->cw = (fmt->width + (1 << fmt->subsampling_w) - 1) >> fmt->subsampling_w;
@@ -420,7 +427,9 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     Slot sJxx = take(L * 4, guided), sJxy = take(L * 4, guided), sJyy = take(L * 4, guided);
     Slot sLc = take(C * 4, guided), sMs = take(C * 4, guided && p.ms > 0.0);
     const bool sparse = guided && p.sparse;
-    Slot sSeed = take(L, sparse), sMtmp = take(L, sparse), sMask = take(L, sparse), sCmask = take(C, sparse);
+    const size_t maskBytes = size_t((sw + 31) / 32) * 4 * sh;
+    Slot sSeed = take(L, sparse), sMtmp = take(maskBytes, sparse), sMask = take(maskBytes, sparse);
+    Slot sCmask = take(C, sparse);
     Slot sOU = take(O * 4), sOV = take(O * 4);
     Slot sLumaTmp = take(size_t(p.outW) * sh * 4, !sameSize && !p.k.radial);  // luma / detail resize
     Slot sCnt = take(kCntCount * sizeof(unsigned long long));
@@ -604,7 +613,10 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.V = packedV ? (const float *)t.in[2].data : ws.Vw;
     J.jxx = ws.jxx; J.jxy = ws.jxy; J.jyy = ws.jyy;
     J.lc = ws.lc; J.ms = ws.ms;
-    J.seed = ws.seed; J.mtmp = ws.mtmp; J.mask = ws.mask; J.cmask = ws.cmask;
+    J.seed = ws.seed; J.cmask = ws.cmask;
+    J.mtmp = reinterpret_cast<uint32_t *>(ws.mtmp);
+    J.mask = reinterpret_cast<uint32_t *>(ws.mask);
+    J.maskWords = (F.sw + 31) / 32;
     J.oU = ws.oU; J.oV = ws.oV; J.lumaTmp = ws.lumaTmp;
     J.counters = ws.counters;
     J.uvd = ws.uvd;
@@ -652,7 +664,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
 // stage scheduler
 // ---------------------------------------------------------------------------
 enum StageId : int {
-    S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_LC, S_DIL_H, S_DIL_V,
+    S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_DIL_H, S_DIL_V,
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
     S_YC, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
@@ -666,7 +678,7 @@ int stageCount() { return S_N; }
 const char *stageName(int s) {
     static const char *names[S_N] = {
         "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
-        "buildGuideMaps_tensor", "buildGuideMaps_lc", "buildTrustMask_h", "buildTrustMask_v",
+        "buildGuideMaps_tensor", "buildTrustMask_h", "buildTrustMask_v",
         "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
         "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain",
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
@@ -752,16 +764,15 @@ static int stageTilesShaped(const FrameJob &J, int s) {
         return (J.guided && J.algo == 6 && pass < J.nyqX + J.nyqY) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
     }
     switch (s) {
-    case S_CONVERT: return cdiv(J.sw, 32) * cdiv(J.sh, 8);
+    case S_CONVERT: return convertBlocks(J.sw, J.sh) + convertBlocks(J.cw, J.ch);
     case S_LUMA_RADIAL: return (resize && J.writeLuma && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_LUMA_H: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_LUMA_V: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
-    case S_TENSOR: return J.guided ? cdiv(J.sw, 32) * cdiv(J.sh, 16) : 0;
-    case S_LC: return J.guided ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_DIL_H: return J.sparse ? cdiv(J.sw, 1024) * J.sh : 0;
-    case S_DIL_V: return J.sparse ? cdiv(J.sw, 32) * cdiv(J.sh, 128) : 0;
-    case S_MARK: return (J.sparse || J.listed) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
-    case S_COUNT: return J.sparse ? cdiv(J.sw * J.sh, 1024) : 0;
+    case S_TENSOR: return J.guided ? cdiv(J.sw, kTensorCols * kTensorWarps) * cdiv(J.sh, kTensorRows) : 0;
+    case S_DIL_H: return J.sparse ? J.sh : 0;
+    case S_DIL_V: return J.sparse ? cdiv(J.maskWords, 32) * cdiv(J.sh, 8) : 0;
+    case S_MARK: return (J.sparse || J.listed) ? cdiv(J.H * cdiv(J.W, 32), 256) : 0;
+    case S_COUNT: return J.sparse ? cdiv(J.cw * J.ch, kCountChunk) : 0;
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_HPASS: return (J.hTab && !J.radial && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
@@ -822,15 +833,14 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
         kernel<<<plan.totals[s], block, smem, stream>>>(dJobs, pre(s), n);
         ++launches;
     };
-    go(S_CONVERT, k_convert, b32x8);
+    go(S_CONVERT, k_convert, dim3(kConvertWarps * 32));
     go(S_LUMA_RADIAL, k_luma_radial, b32x8);
     go(S_LUMA_H, k_luma_h, b32x8);
     go(S_LUMA_V, k_luma_v, b32x8);
-    go(S_TENSOR, k_tensor, dim3(32, 8));
-    go(S_LC, k_lc, b32x8);
-    go(S_DIL_H, k_dilate_h, dim3(256));
-    go(S_DIL_V, k_dilate_v, dim3(32), size_t(128 + 2 * plan.maxDil) * 32);
-    go(S_MARK, k_mark_chroma, b32x8);
+    go(S_TENSOR, k_tensor, dim3(kTensorWarps * 32));
+    go(S_DIL_H, k_dilate_h, dim3(128));
+    go(S_DIL_V, k_dilate_v, dim3(32, 8));
+    go(S_MARK, k_mark_chroma, dim3(256));
     go(S_COUNT, k_count, dim3(256));
     go(S_GATE, k_gate, b32x8);
     go(S_LGF_DENSE, k_lgf, b32x8);

@@ -99,7 +99,9 @@ struct FrameJob {
     float *Yw, *Uw, *Vw;               // conversion targets (== Y/U/V when converted)
     float *jxx, *jxy, *jyy;            // sw x sh
     float *lc, *ms;                    // cw x ch
-    uint8_t *seed, *mtmp, *mask;       // sw x sh
+    uint8_t *seed;                     // sw x sh trust seed (0/1 bytes)
+    uint32_t *mtmp, *mask;             // sw x sh bits: maskWords words per row
+    int maskWords;                     // (sw + 31) / 32
     uint8_t *cmask;                    // cw x ch
     float *oU, *oV;                    // W x H float output planes
     float *lumaTmp;                    // W x sh luma resize intermediate
@@ -170,6 +172,11 @@ __device__ __forceinline__ float rcpAtLeastOne(float x) {
         return __fmaf_rn(y, e, y);
     }
     return 1.0f / x;
+}
+
+// Dilated trust mask bit of luma sample (x, y).
+__device__ __forceinline__ uint32_t maskAt(const FrameJob &J, int x, int y) {
+    return (__ldg(J.mask + (size_t)y * J.maskWords + (x >> 5)) >> (x & 31)) & 1u;
 }
 
 // Block -> frame by binary search over the stage prefix table.

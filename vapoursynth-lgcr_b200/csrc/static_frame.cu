@@ -150,8 +150,9 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     const size_t oJxx = guided ? take(L * 4) : 0, oJxy = guided ? take(L * 4) : 0;
     const size_t oJyy = guided ? take(L * 4) : 0, oLc = guided ? take(C * 4) : 0;
     const size_t oMs = (guided && q.ms > 0.0) ? take(C * 4) : 0;
-    const size_t oSeed = sparse ? take(L) : 0, oMtmp = sparse ? take(L) : 0;
-    const size_t oMask = sparse ? take(L) : 0, oCmask = sparse ? take(C) : 0;
+    const size_t maskBytes = size_t((F.sw + 31) / 32) * 4 * F.sh;
+    const size_t oSeed = sparse ? take(L) : 0, oMtmp = sparse ? take(maskBytes) : 0;
+    const size_t oMask = sparse ? take(maskBytes) : 0, oCmask = sparse ? take(C) : 0;
     const size_t oLumaTmp = (!sameSize && !q.k.radial) ? take(size_t(q.outW) * F.sh * 4) : 0;
     const size_t oUvd = take(C * 16);
     const size_t oList = guided ? take(size_t(q.outW) * q.outH * 4) : 0;
