@@ -72,6 +72,7 @@ struct DeviceTables {
     const int *bmStartsX = nullptr, *bmStartsY = nullptr;
     int bmAnchorsX = 0, bmAnchorsY = 0;
     int axSup = 0, aySup = 0;
+    int plainMaxRows = 0;               // most chroma rows one k_plain block reads
 };
 
 struct Filter;

@@ -45,8 +45,10 @@ __device__ __forceinline__ void storeRaw(void *plane, long long pitch, int kind,
 
 __global__ void __launch_bounds__(kConvertWarps * 32)
 k_convert(LGCR_STAGE_ARGS) {
+    __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
     const int tile = blockIdx.x - tileStart[f];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lumaBlocks = convertLumaBlocks(J.sw, J.sh);

@@ -24,12 +24,65 @@
 namespace lgcr_b200 {
 
 // ---------------------------------------------------------------------------
-// horizontal table: hu hv mnU mxU | mnV mxV mnL mxL
+// horizontal table: hu hv mnU mxU | mnV mxV mnL mxL per (output column,
+// chroma row) over the column's active taps
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t maskBits(const uint8_t *am, int n) {
+    uint32_t m = 0;
+    for (int i = 0; i < n; ++i)
+        m |= (__ldg(am + i) != 0 ? 1u : 0u) << i;
+    return m;
+}
+
+// Tap data of one output column (start, activity bits, FP64 weights), loaded
+// once and reused for every chroma row the column is evaluated on.
 template <int SUP>
-__device__ __forceinline__ void hpassAt(const FrameJob &J, int ox, int sy) {
+struct HColumn {
+    int tx0;
+    uint32_t active;
+    double w[SUP];
+    __device__ __forceinline__ void load(const AxisView &ax, int ox) {
+        tx0 = __ldg(ax.start + ox);
+        active = maskBits(ax.am + (size_t)ox * SUP, SUP);
+#pragma unroll
+        for (int i = 0; i < SUP; ++i)
+            w[i] = __ldg(ax.wd + (size_t)ox * SUP + i);
+    }
+};
+
+template <int SUP>
+__device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &col, int sy, float4 &ea,
+                                       float4 &eb) {
+    const int cw = J.cw;
+    const double2 *uv = reinterpret_cast<const double2 *>(J.uvd) + (size_t)sy * cw;
+    const float *lrow = J.lc ? J.lc + (size_t)sy * cw : nullptr;
+    double hU = 0.0, hV = 0.0;
+    double mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+    float mnL = 1e30f, mxL = -1e30f;
+#pragma unroll
+    for (int i = 0; i < SUP; ++i) {
+        if (!((col.active >> i) & 1u))
+            continue;
+        const int x = J.noClampX ? col.tx0 + i : iclamp(col.tx0 + i, 0, cw - 1);
+        const double2 p = __ldg(uv + x);
+        const double w = col.w[i];
+        hU = fma(w, p.x, hU);
+        hV = fma(w, p.y, hV);
+        mnU = smin(mnU, p.x); mxU = smax(mxU, p.x);
+        mnV = smin(mnV, p.y); mxV = smax(mxV, p.y);
+        if (lrow) {
+            const float l = ldf(lrow + x);
+            mnL = smin(mnL, l); mxL = smax(mxL, l);
+        }
+    }
+    ea = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
+    eb = make_float4((float)mnV, (float)mxV, mnL, mxL);
+}
+
+// Any support (activity read per tap).
+__device__ __forceinline__ void hEntryGeneric(const FrameJob &J, int ox, int sy, float4 &ea, float4 &eb) {
     const AxisView &ax = J.ax;
-    const int n = SUP > 0 ? SUP : ax.sup;
+    const int n = ax.sup;
     const int cw = J.cw;
     const int tx0 = __ldg(ax.start + ox);
     const double *wx = ax.wd + (size_t)ox * ax.sup;
@@ -39,7 +92,6 @@ __device__ __forceinline__ void hpassAt(const FrameJob &J, int ox, int sy) {
     double hU = 0.0, hV = 0.0;
     double mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
     float mnL = 1e30f, mxL = -1e30f;
-#pragma unroll
     for (int i = 0; i < n; ++i) {
         if (__ldg(amx + i) == 0)
             continue;
@@ -55,11 +107,19 @@ __device__ __forceinline__ void hpassAt(const FrameJob &J, int ox, int sy) {
             mnL = smin(mnL, l); mxL = smax(mxL, l);
         }
     }
-    float4 *o = reinterpret_cast<float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
-    o[0] = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
-    o[1] = make_float4((float)mnV, (float)mxV, mnL, mxL);
+    ea = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
+    eb = make_float4((float)mnV, (float)mxV, mnL, mxL);
 }
 
+__device__ __forceinline__ void storeEntry(const FrameJob &J, int ox, int sy, const float4 &ea,
+                                           const float4 &eb) {
+    float4 *o = reinterpret_cast<float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
+    o[0] = ea;
+    o[1] = eb;
+}
+
+// Standalone horizontal pass (frames whose plain blocks cannot stage their
+// rows in shared memory).
 __global__ void __launch_bounds__(256)
 k_hpass(LGCR_STAGE_ARGS) {
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -68,12 +128,14 @@ k_hpass(LGCR_STAGE_ARGS) {
     tile32x8(blockIdx.x - tileStart[f], J.W, ox, sy);
     if (ox >= J.W || sy >= J.ch)
         return;
+    float4 a, b;
     switch (J.ax.sup) {
-    case 4: hpassAt<4>(J, ox, sy); break;
-    case 6: hpassAt<6>(J, ox, sy); break;
-    case 8: hpassAt<8>(J, ox, sy); break;
-    default: hpassAt<0>(J, ox, sy); break;
+    case 4: { HColumn<4> c; c.load(J.ax, ox); hEntry<4>(J, c, sy, a, b); break; }
+    case 6: { HColumn<6> c; c.load(J.ax, ox); hEntry<6>(J, c, sy, a, b); break; }
+    case 8: { HColumn<8> c; c.load(J.ax, ox); hEntry<8>(J, c, sy, a, b); break; }
+    default: hEntryGeneric(J, ox, sy, a, b); break;
     }
+    storeEntry(J, ox, sy, a, b);
 }
 
 // Plain separable value from the horizontal table (vertical pass).
@@ -156,9 +218,11 @@ __device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u,
 }
 
 // Vertical pass over table rows staged in shared memory: same arithmetic and
-// order as plainFromTableT, rows indexed relative to the staged block.
+// order as plainFromTableT, rows indexed relative to the staged block. The
+// horizontal sums are staged already widened to double (the float-rounded
+// ring value, as the reference multiplies it in double).
 template <int SUP>
-__device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 (*sHV)[32],
+__device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2 (*sHV)[32],
                                                 const float2 (*sU)[32], const float2 (*sV)[32],
                                                 int syLo, int lx, int ox, int oy, float &outU,
                                                 float &outV) {
@@ -174,10 +238,11 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 
         if (__ldg(amy + j) == 0)
             continue;
         const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
-        const float2 h = sHV[r][lx], eu = sU[r][lx], ev = sV[r][lx];
+        const double2 h = sHV[r][lx];
+        const float2 eu = sU[r][lx], ev = sV[r][lx];
         const double w = __ldg(wy + j);
-        vU = fma(w, (double)h.x, vU);
-        vV = fma(w, (double)h.y, vV);
+        vU = fma(w, h.x, vU);
+        vV = fma(w, h.y, vV);
         mnU = smin(mnU, eu.x); mxU = smax(mxU, eu.y);
         mnV = smin(mnV, ev.x); mxV = smax(mxV, ev.y);
     }
@@ -199,65 +264,215 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 
     outV = (float)vV;
 }
 
+// Per-row vertical tap data of one k_plain block, staged once for the
+// block's kPlainRows output rows (supports up to 8 taps).
+struct PlainRows {
+    double w[kPlainRows][8];
+    int ty0[kPlainRows];
+    uint32_t act[kPlainRows];
+    float wsum[kPlainRows], wabs[kPlainRows], pos[kPlainRows];
+    uint32_t maskWord[kPlainRows];     // active-pixel bits of the block's 32 columns
+};
+
+// The same vertical pass with the row data from PlainRows and the column
+// data (wsX, waX, posX) held in registers.
+template <int SUP>
+__device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (*sHV)[32],
+                                              const float2 (*sU)[32], const float2 (*sV)[32],
+                                              const PlainRows &R, int k, int syLo, int lx,
+                                              float wsX, float waX, float posX, float &outU,
+                                              float &outV) {
+    const int ty0 = R.ty0[k];
+    const uint32_t act = R.act[k];
+    double vU = 0.0, vV = 0.0;
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((act >> j) & 1u))
+            continue;
+        const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
+        const double2 h = sHV[r][lx];
+        const float2 eu = sU[r][lx], ev = sV[r][lx];
+        const double w = R.w[k][j];
+        vU = fma(w, h.x, vU);
+        vV = fma(w, h.y, vV);
+        mnU = smin(mnU, eu.x); mxU = smax(mxU, eu.y);
+        mnV = smin(mnV, ev.x); mxV = smax(mxV, ev.y);
+    }
+    const double ws = (double)wsX * (double)R.wsum[k];
+    const double wa = (double)waX * (double)R.wabs[k];
+    if (ws > 1e-6 && ws >= 0.05 * wa) {
+        vU /= ws;
+        vV /= ws;
+    } else {
+        vU = bilinearAt(J.U, J.cw, J.ch, posX, R.pos[k]);
+        vV = bilinearAt(J.V, J.cw, J.ch, posX, R.pos[k]);
+    }
+    if (J.clampHull) {
+        vU = sclamp(vU, (double)(mnU - J.margin), (double)(mxU + J.margin));
+        vV = sclamp(vV, (double)(mnV - J.margin), (double)(mxV + J.margin));
+    }
+    outU = (float)vU;
+    outV = (float)vV;
+}
+
+// Horizontal entries of the rows [syLo, syLo + nRows) for output column ox
+// into shared memory; table rows this block owns (sy < syOwnEnd) also go to
+// the frame's horizontal table for the guided pass. Two rows per step keep
+// both rows' loads in flight together.
+__device__ __forceinline__ void putEntry(const FrameJob &J, int ox, int lx, int r, int sy, const float4 &a,
+                                         const float4 &b, int syOwnEnd, bool writeTable,
+                                         double2 (*sHV)[32], float2 (*sU)[32], float2 (*sV)[32]) {
+    sHV[r][lx] = make_double2((double)a.x, (double)a.y);
+    sU[r][lx] = make_float2(a.z, a.w);
+    sV[r][lx] = make_float2(b.x, b.y);
+    if (writeTable && sy < syOwnEnd)
+        storeEntry(J, ox, sy, a, b);
+}
+
+template <int SUP>
+__device__ __forceinline__ void stageRows(const FrameJob &J, int ox, int lx, int syLo, int nRows,
+                                          int syOwnEnd, bool writeTable, double2 (*sHV)[32],
+                                          float2 (*sU)[32], float2 (*sV)[32]) {
+    HColumn<SUP> col;
+    col.load(J.ax, ox);
+    const int step = blockDim.y;
+    int r = threadIdx.y;
+    for (; r + step < nRows; r += 2 * step) {
+        float4 a0, b0, a1, b1;
+        hEntry<SUP>(J, col, syLo + r, a0, b0);
+        hEntry<SUP>(J, col, syLo + r + step, a1, b1);
+        putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, sHV, sU, sV);
+        putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, sHV, sU, sV);
+    }
+    if (r < nRows) {
+        float4 a, b;
+        hEntry<SUP>(J, col, syLo + r, a, b);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sU, sV);
+    }
+}
+
+__device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int lx, int syLo, int nRows,
+                                                 int syOwnEnd, bool writeTable, double2 (*sHV)[32],
+                                                 float2 (*sU)[32], float2 (*sV)[32]) {
+    for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
+        float4 a, b;
+        hEntryGeneric(J, ox, syLo + r, a, b);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sU, sV);
+    }
+}
+
 // Plain stage: every pixel the guided pass does not finalize. A block covers
-// 32 output columns x kPlainRows output rows; for the separable table path
-// it first stages the table rows its windows touch (each row read once per
-// block instead of once per output pixel), then runs the vertical pass from
-// shared memory. Blocks whose rows do not fit (strong vertical downscale)
-// read the table directly.
-__global__ void __launch_bounds__(256)
+// 32 output columns x kPlainRows output rows. For the separable kernels it
+// needs the horizontal entries of the chroma rows its windows touch:
+//  * fused frames (every block's rows fit in shared memory) compute them
+//    here from the chroma planes (the reference's ring rows), and write the
+//    rows the block owns to the horizontal table when the guided pass reads
+//    it (chroma row sy is owned by the last block whose rows start at or
+//    before sy, so every row some window reads is written exactly once);
+//  * other frames stage rows of the table written by k_hpass, or read the
+//    table directly when the rows do not fit (strong vertical downscale).
+// The vertical pass then runs from shared memory, with the per-row tap data
+// and active-pixel bits staged once per block for supports up to 8.
+__global__ void __launch_bounds__(256, 4)
 k_plain(LGCR_STAGE_ARGS) {
-    __shared__ float2 sHV[kPlainStagedRows][32];
+    __shared__ double2 sHV[kPlainStagedRows][32];
     __shared__ float2 sU[kPlainStagedRows][32];
     __shared__ float2 sV[kPlainStagedRows][32];
+    __shared__ PlainRows R;
+    __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
     const int tile = blockIdx.x - tileStart[f];
     const int tilesX = (J.W + 31) >> 5;
     const int colBase = (tile % tilesX) * 32;
     const int oy0 = (tile / tilesX) * kPlainRows;
+    const int rowsHere = min(kPlainRows, J.H - oy0);
     const int lx = threadIdx.x;
     const int ox = colBase + lx;
-    const bool table = !J.radial && J.kernel != 0 && J.hTab;
+    const int tid = threadIdx.y * 32 + lx;
+    const bool separable = !J.radial && J.kernel != 0;
+    const bool fused = J.plainFused && (separable || J.listed);
+    const bool table = separable && (J.hTab || fused);
+    const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
+    const bool skipListed = J.listed && !floatSelector;
     int syLo = 0, nRows = 0;
-    if (table) {
-        const int oyLast = min(oy0 + kPlainRows, J.H) - 1;
+    if (table || fused) {
+        const int oyLast = oy0 + rowsHere - 1;
         syLo = iclamp(__ldg(J.ay.start + oy0), 0, J.ch - 1);
         const int syHi = iclamp(__ldg(J.ay.start + oyLast) + J.ay.sup - 1, 0, J.ch - 1);
         nRows = syHi - syLo + 1;
     }
-    const bool staged = table && nRows <= kPlainStagedRows;
-    if (staged) {
+    const bool staged = (table || fused) && nRows <= kPlainStagedRows;
+    const int sup = J.ay.sup;
+    const bool rowTables = table && staged && sup <= 8;
+    if (rowTables) {
+        for (int i = tid; i < rowsHere * sup; i += 256) {
+            const int k = i / sup, j = i - k * sup;
+            R.w[k][j] = __ldg(J.ay.wd + (size_t)(oy0 + k) * sup + j);
+        }
+        if (tid < rowsHere) {
+            const int oy = oy0 + tid;
+            R.ty0[tid] = __ldg(J.ay.start + oy);
+            R.act[tid] = maskBits(J.ay.am + (size_t)oy * sup, sup);
+            R.wsum[tid] = __ldg(J.ay.wsum + oy);
+            R.wabs[tid] = __ldg(J.ay.wabs + oy);
+            R.pos[tid] = __ldg(J.ay.pos + oy);
+        }
+    }
+    const bool maskWords = skipListed && J.sparse && J.sameSize;
+    if (maskWords && tid < rowsHere)
+        R.maskWord[tid] = __ldg(J.mask + (size_t)(oy0 + tid) * J.maskWords + (colBase >> 5));
+    if (fused) {
+        // rows from the next block's first row on belong to the next block
+        const int syOwnEnd = (oy0 + kPlainRows < J.H)
+            ? iclamp(__ldg(J.ay.start + oy0 + kPlainRows), 0, J.ch - 1) : J.ch;
+        const bool writeTable = J.listed && J.hTab;
         if (ox < J.W) {
-            for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
-                const float4 *h =
-                    reinterpret_cast<const float4 *>(J.hTab + ((size_t)(syLo + r) * J.W + ox) * 8);
-                const float4 a = __ldg(h), b = __ldg(h + 1);
-                sHV[r][lx] = make_float2(a.x, a.y);
-                sU[r][lx] = make_float2(a.z, a.w);
-                sV[r][lx] = make_float2(b.x, b.y);
+            switch (J.ax.sup) {
+            case 4: stageRows<4>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
+            case 6: stageRows<6>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
+            case 8: stageRows<8>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
+            default: stageRowsGeneric(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
             }
         }
-        __syncthreads();
+    } else if (staged && ox < J.W) {
+        for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
+            const float4 *h =
+                reinterpret_cast<const float4 *>(J.hTab + ((size_t)(syLo + r) * J.W + ox) * 8);
+            const float4 a = __ldg(h), b = __ldg(h + 1);
+            sHV[r][lx] = make_double2((double)a.x, (double)a.y);
+            sU[r][lx] = make_float2(a.z, a.w);
+            sV[r][lx] = make_float2(b.x, b.y);
+        }
     }
+    __syncthreads();
     if (ox >= J.W)
         return;
-    const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
-    for (int k = threadIdx.y; k < kPlainRows; k += blockDim.y) {
+    float wsX = 0.0f, waX = 0.0f, posX = 0.0f;
+    if (rowTables) {
+        wsX = __ldg(J.ax.wsum + ox);
+        waX = __ldg(J.ax.wabs + ox);
+        posX = __ldg(J.ax.pos + ox);
+    }
+    for (int k = threadIdx.y; k < rowsHere; k += blockDim.y) {
         const int oy = oy0 + k;
-        if (oy >= J.H)
-            break;
         // listed pixels of algo 2 and integer algo 4 are written by k_guided
-        if (J.listed && !floatSelector && pixelActive(J, ox, oy))
-            continue;
+        if (skipListed) {
+            const bool act = maskWords ? ((R.maskWord[k] >> lx) & 1u) != 0 : pixelActive(J, ox, oy);
+            if (act)
+                continue;
+        }
         float u, v;
-        if (staged) {
-            switch (J.ay.sup) {
-            case 4: plainFromStaged<4>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
-            case 6: plainFromStaged<6>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
-            case 8: plainFromStaged<8>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
-            default: plainFromStaged<0>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v); break;
+        if (rowTables) {
+            switch (sup) {
+            case 4: plainFromRows<4>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+            case 6: plainFromRows<6>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+            default: plainFromRows<8>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
             }
+        } else if (table && staged) {
+            plainFromStaged<0>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v);
         } else {
             plainPixel(J, ox, oy, u, v);
         }
@@ -374,13 +589,6 @@ __device__ __forceinline__ void tapsGeneric(const FrameJob &J, const TapCtx &c, 
             tap(c, o, dxf, dy_ny, dy_nx, wx, a);
         }
     }
-}
-
-__device__ __forceinline__ uint32_t maskBits(const uint8_t *am, int n) {
-    uint32_t m = 0;
-    for (int i = 0; i < n; ++i)
-        m |= (__ldg(am + i) != 0 ? 1u : 0u) << i;
-    return m;
 }
 
 // Window extrema of U, V and lc over the active taps from the table rows:

@@ -366,6 +366,12 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
     t->ay = axisView(t->arena, oay);
     t->axSup = ax.sup;
     t->aySup = ay.sup;
+    for (int oy0 = 0; oy0 < p.outH; oy0 += kPlainRows) {
+        const int oyLast = std::min(oy0 + kPlainRows, p.outH) - 1;
+        const int lo = std::clamp(ay.start[oy0], 0, ch - 1);
+        const int hi = std::clamp(ay.start[oyLast] + ay.sup - 1, 0, ch - 1);
+        t->plainMaxRows = std::max(t->plainMaxRows, hi - lo + 1);
+    }
     if (p.k.radial)
         t->rad = radialView(t->arena, orad);
     if (!sameSize && !p.k.radial) {
@@ -623,6 +629,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.hTab = ws.hTab;
     J.actList = ws.actList;
     J.listed = J.guided && (p.algo == 2 || p.algo == 4);
+    J.plainFused = (J.hTab && !J.radial && T.plainMaxRows <= kPlainStagedRows) ? 1 : 0;
     {
         // every tap index in range: starts lie in [0, srcChromaN - sup] and the
         // integer-ratio chroma count equals the plane size
@@ -775,7 +782,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_COUNT: return J.sparse ? cdiv(J.cw * J.ch, kCountChunk) : 0;
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_HPASS: return (J.hTab && !J.radial && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
+    case S_HPASS: return (J.hTab && !J.radial && !J.plainFused && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
     case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, kPlainRows);
     case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC:

@@ -58,7 +58,7 @@ enum Counter : int {
     kCntCount = 8
 };
 
-struct FrameJob {
+struct __align__(16) FrameJob {
     // geometry
     int sw, sh, cw, ch, W, H;
     double rw, rh;
@@ -110,6 +110,7 @@ struct FrameJob {
     double *uvd;                       // cw x ch x 2: (u, v) in FP64
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
+    int plainFused;                    // k_plain computes its horizontal rows itself
     int noClampX, noClampY;            // every chroma tap index is in range
     // algo 6 / algo 4 / bm workspaces
     float *aff;                        // 9 chroma planes: aU aV g mnU mxU mnV mxV rng dgl
@@ -177,6 +178,19 @@ __device__ __forceinline__ float rcpAtLeastOne(float x) {
 // Dilated trust mask bit of luma sample (x, y).
 __device__ __forceinline__ uint32_t maskAt(const FrameJob &J, int x, int y) {
     return (__ldg(J.mask + (size_t)y * J.maskWords + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// Shared-memory copy of one frame's job for the whole block. Kernels that
+// read FrameJob fields inside loops with global stores read them from this
+// copy, so the fields are not reloaded from global memory after each store.
+__device__ __forceinline__ void stageJob(const FrameJob *__restrict__ jobs, int f, FrameJob &s) {
+    const int4 *src = reinterpret_cast<const int4 *>(jobs + f);
+    int4 *dst = reinterpret_cast<int4 *>(&s);
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    for (int i = tid; i < (int)(sizeof(FrameJob) / 16); i += nthreads)
+        dst[i] = __ldg(src + i);
+    __syncthreads();
 }
 
 // Block -> frame by binary search over the stage prefix table.
