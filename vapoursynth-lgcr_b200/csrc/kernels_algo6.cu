@@ -61,8 +61,10 @@ __global__ void k_yc_h(LGCR_STAGE_ARGS) {
 // 5x5 affine statistics per chroma sample (active samples when sparse).
 __global__ void __launch_bounds__(256)
 k_affine(LGCR_STAGE_ARGS) {
+    __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
     int x, y;
     tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
     const int w = J.cw, h = J.ch;

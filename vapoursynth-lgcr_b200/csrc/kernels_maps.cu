@@ -444,8 +444,10 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     __shared__ float src[3][GT_Y + 2 * GH + 2][GT_X + 2 * GH + 2];
     __shared__ float gx[3][GT_Y + 2 * GH][GT_X + 2 * GH];
     __shared__ float gy[3][GT_Y + 2 * GH][GT_X + 2 * GH];
+    __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
     const int tile = blockIdx.x - tileStart[f];
     const int w = J.cw, h = J.ch;
     const int tilesX = (w + GT_X - 1) / GT_X;
