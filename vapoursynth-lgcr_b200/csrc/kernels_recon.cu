@@ -50,7 +50,7 @@ struct HColumn {
     }
 };
 
-template <int SUP>
+template <int SUP, bool NOCLAMP>
 __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &col, int sy, float4 &ea,
                                        float4 &eb) {
     const int cw = J.cw;
@@ -63,7 +63,7 @@ __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &co
     for (int i = 0; i < SUP; ++i) {
         if (!((col.active >> i) & 1u))
             continue;
-        const int x = J.noClampX ? col.tx0 + i : iclamp(col.tx0 + i, 0, cw - 1);
+        const int x = NOCLAMP ? col.tx0 + i : iclamp(col.tx0 + i, 0, cw - 1);
         const double2 p = __ldg(uv + x);
         const double w = col.w[i];
         hU = fma(w, p.x, hU);
@@ -130,9 +130,9 @@ k_hpass(LGCR_STAGE_ARGS) {
         return;
     float4 a, b;
     switch (J.ax.sup) {
-    case 4: { HColumn<4> c; c.load(J.ax, ox); hEntry<4>(J, c, sy, a, b); break; }
-    case 6: { HColumn<6> c; c.load(J.ax, ox); hEntry<6>(J, c, sy, a, b); break; }
-    case 8: { HColumn<8> c; c.load(J.ax, ox); hEntry<8>(J, c, sy, a, b); break; }
+    case 4: { HColumn<4> c; c.load(J.ax, ox); if (J.noClampX) hEntry<4, true>(J, c, sy, a, b); else hEntry<4, false>(J, c, sy, a, b); break; }
+    case 6: { HColumn<6> c; c.load(J.ax, ox); if (J.noClampX) hEntry<6, true>(J, c, sy, a, b); else hEntry<6, false>(J, c, sy, a, b); break; }
+    case 8: { HColumn<8> c; c.load(J.ax, ox); if (J.noClampX) hEntry<8, true>(J, c, sy, a, b); else hEntry<8, false>(J, c, sy, a, b); break; }
     default: hEntryGeneric(J, ox, sy, a, b); break;
     }
     storeEntry(J, ox, sy, a, b);
@@ -223,9 +223,8 @@ __device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u,
 // ring value, as the reference multiplies it in double).
 template <int SUP>
 __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2 (*sHV)[32],
-                                                const float2 (*sU)[32], const float2 (*sV)[32],
-                                                int syLo, int lx, int ox, int oy, float &outU,
-                                                float &outV) {
+                                                const float4 (*sE)[32], int syLo, int lx, int ox,
+                                                int oy, float &outU, float &outV) {
     const AxisView &ax = J.ax, &ay = J.ay;
     const int n = SUP > 0 ? SUP : ay.sup;
     const int ty0 = __ldg(ay.start + oy);
@@ -239,12 +238,12 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2
             continue;
         const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
         const double2 h = sHV[r][lx];
-        const float2 eu = sU[r][lx], ev = sV[r][lx];
+        const float4 e = sE[r][lx];
         const double w = __ldg(wy + j);
         vU = fma(w, h.x, vU);
         vV = fma(w, h.y, vV);
-        mnU = smin(mnU, eu.x); mxU = smax(mxU, eu.y);
-        mnV = smin(mnV, ev.x); mxV = smax(mxV, ev.y);
+        mnU = smin(mnU, e.x); mxU = smax(mxU, e.y);
+        mnV = smin(mnV, e.z); mxV = smax(mxV, e.w);
     }
     const double ws = (double)__ldg(ax.wsum + ox) * (double)__ldg(ay.wsum + oy);
     const double wa = (double)__ldg(ax.wabs + ox) * (double)__ldg(ay.wabs + oy);
@@ -276,12 +275,11 @@ struct PlainRows {
 
 // The same vertical pass with the row data from PlainRows and the column
 // data (wsX, waX, posX) held in registers.
-template <int SUP>
+template <int SUP, bool NOCLAMP>
 __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (*sHV)[32],
-                                              const float2 (*sU)[32], const float2 (*sV)[32],
-                                              const PlainRows &R, int k, int syLo, int lx,
-                                              float wsX, float waX, float posX, float &outU,
-                                              float &outV) {
+                                              const float4 (*sE)[32], const PlainRows &R, int k,
+                                              int syLo, int lx, float wsX, float waX, float posX,
+                                              float &outU, float &outV) {
     const int ty0 = R.ty0[k];
     const uint32_t act = R.act[k];
     double vU = 0.0, vV = 0.0;
@@ -290,14 +288,14 @@ __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (
     for (int j = 0; j < SUP; ++j) {
         if (!((act >> j) & 1u))
             continue;
-        const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
+        const int r = (NOCLAMP ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
         const double2 h = sHV[r][lx];
-        const float2 eu = sU[r][lx], ev = sV[r][lx];
+        const float4 e = sE[r][lx];
         const double w = R.w[k][j];
         vU = fma(w, h.x, vU);
         vV = fma(w, h.y, vV);
-        mnU = smin(mnU, eu.x); mxU = smax(mxU, eu.y);
-        mnV = smin(mnV, ev.x); mxV = smax(mxV, ev.y);
+        mnU = smin(mnU, e.x); mxU = smax(mxU, e.y);
+        mnV = smin(mnV, e.z); mxV = smax(mxV, e.w);
     }
     const double ws = (double)wsX * (double)R.wsum[k];
     const double wa = (double)waX * (double)R.wabs[k];
@@ -322,43 +320,52 @@ __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (
 // both rows' loads in flight together.
 __device__ __forceinline__ void putEntry(const FrameJob &J, int ox, int lx, int r, int sy, const float4 &a,
                                          const float4 &b, int syOwnEnd, bool writeTable,
-                                         double2 (*sHV)[32], float2 (*sU)[32], float2 (*sV)[32]) {
+                                         double2 (*sHV)[32], float4 (*sE)[32]) {
     sHV[r][lx] = make_double2((double)a.x, (double)a.y);
-    sU[r][lx] = make_float2(a.z, a.w);
-    sV[r][lx] = make_float2(b.x, b.y);
+    sE[r][lx] = make_float4(a.z, a.w, b.x, b.y);
     if (writeTable && sy < syOwnEnd)
         storeEntry(J, ox, sy, a, b);
+}
+
+template <int SUP, bool NOCLAMP>
+__device__ __forceinline__ void stageRowsT(const FrameJob &J, const HColumn<SUP> &col, int ox, int lx,
+                                           int syLo, int nRows, int syOwnEnd, bool writeTable,
+                                           double2 (*sHV)[32], float4 (*sE)[32]) {
+    const int step = blockDim.y;
+    int r = threadIdx.y;
+    for (; r + step < nRows; r += 2 * step) {
+        float4 a0, b0, a1, b1;
+        hEntry<SUP, NOCLAMP>(J, col, syLo + r, a0, b0);
+        hEntry<SUP, NOCLAMP>(J, col, syLo + r + step, a1, b1);
+        putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, sHV, sE);
+        putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, sHV, sE);
+    }
+    if (r < nRows) {
+        float4 a, b;
+        hEntry<SUP, NOCLAMP>(J, col, syLo + r, a, b);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sE);
+    }
 }
 
 template <int SUP>
 __device__ __forceinline__ void stageRows(const FrameJob &J, int ox, int lx, int syLo, int nRows,
                                           int syOwnEnd, bool writeTable, double2 (*sHV)[32],
-                                          float2 (*sU)[32], float2 (*sV)[32]) {
+                                          float4 (*sE)[32]) {
     HColumn<SUP> col;
     col.load(J.ax, ox);
-    const int step = blockDim.y;
-    int r = threadIdx.y;
-    for (; r + step < nRows; r += 2 * step) {
-        float4 a0, b0, a1, b1;
-        hEntry<SUP>(J, col, syLo + r, a0, b0);
-        hEntry<SUP>(J, col, syLo + r + step, a1, b1);
-        putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, sHV, sU, sV);
-        putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, sHV, sU, sV);
-    }
-    if (r < nRows) {
-        float4 a, b;
-        hEntry<SUP>(J, col, syLo + r, a, b);
-        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sU, sV);
-    }
+    if (J.noClampX)
+        stageRowsT<SUP, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE);
+    else
+        stageRowsT<SUP, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE);
 }
 
 __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int lx, int syLo, int nRows,
                                                  int syOwnEnd, bool writeTable, double2 (*sHV)[32],
-                                                 float2 (*sU)[32], float2 (*sV)[32]) {
+                                                 float4 (*sE)[32]) {
     for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
         float4 a, b;
         hEntryGeneric(J, ox, syLo + r, a, b);
-        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sU, sV);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sE);
     }
 }
 
@@ -377,8 +384,7 @@ __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int 
 __global__ void __launch_bounds__(256, 4)
 k_plain(LGCR_STAGE_ARGS) {
     __shared__ double2 sHV[kPlainStagedRows][32];
-    __shared__ float2 sU[kPlainStagedRows][32];
-    __shared__ float2 sV[kPlainStagedRows][32];
+    __shared__ float4 sE[kPlainStagedRows][32];      // mnU mxU mnV mxV
     __shared__ PlainRows R;
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -431,10 +437,10 @@ k_plain(LGCR_STAGE_ARGS) {
         const bool writeTable = J.listed && J.hTab;
         if (ox < J.W) {
             switch (J.ax.sup) {
-            case 4: stageRows<4>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
-            case 6: stageRows<6>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
-            case 8: stageRows<8>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
-            default: stageRowsGeneric(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sU, sV); break;
+            case 4: stageRows<4>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
+            case 6: stageRows<6>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
+            case 8: stageRows<8>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
+            default: stageRowsGeneric(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
             }
         }
     } else if (staged && ox < J.W) {
@@ -443,8 +449,7 @@ k_plain(LGCR_STAGE_ARGS) {
                 reinterpret_cast<const float4 *>(J.hTab + ((size_t)(syLo + r) * J.W + ox) * 8);
             const float4 a = __ldg(h), b = __ldg(h + 1);
             sHV[r][lx] = make_double2((double)a.x, (double)a.y);
-            sU[r][lx] = make_float2(a.z, a.w);
-            sV[r][lx] = make_float2(b.x, b.y);
+            sE[r][lx] = make_float4(a.z, a.w, b.x, b.y);
         }
     }
     __syncthreads();
@@ -466,13 +471,21 @@ k_plain(LGCR_STAGE_ARGS) {
         }
         float u, v;
         if (rowTables) {
-            switch (sup) {
-            case 4: plainFromRows<4>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
-            case 6: plainFromRows<6>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
-            default: plainFromRows<8>(J, sHV, sU, sV, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+            if (J.noClampY) {
+                switch (sup) {
+                case 4: plainFromRows<4, true>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                case 6: plainFromRows<6, true>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                default: plainFromRows<8, true>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                }
+            } else {
+                switch (sup) {
+                case 4: plainFromRows<4, false>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                case 6: plainFromRows<6, false>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                default: plainFromRows<8, false>(J, sHV, sE, R, k, syLo, lx, wsX, waX, posX, u, v); break;
+                }
             }
         } else if (table && staged) {
-            plainFromStaged<0>(J, sHV, sU, sV, syLo, lx, ox, oy, u, v);
+            plainFromStaged<0>(J, sHV, sE, syLo, lx, ox, oy, u, v);
         } else {
             plainPixel(J, ox, oy, u, v);
         }
