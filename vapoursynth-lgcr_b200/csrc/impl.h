@@ -73,6 +73,8 @@ struct DeviceTables {
     int bmAnchorsX = 0, bmAnchorsY = 0;
     int axSup = 0, aySup = 0;
     int plainMaxRows = 0;               // most chroma rows one k_plain block reads
+    int detailMaxRows = 0;              // most chroma rows one k_detail_map block reads
+    int sAxSup = 0, sAySup = 0;         // source-grid axis supports (algo 6)
 };
 
 struct Filter;

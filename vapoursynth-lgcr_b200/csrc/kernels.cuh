@@ -58,6 +58,9 @@ __global__ void k_affine(LGCR_STAGE_ARGS);
 __global__ void k_detail_hpass(LGCR_STAGE_ARGS);
 __global__ void k_detail_plain(LGCR_STAGE_ARGS);
 __global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass);
+// k_detail_map: output samples per block side (32 computed with the halo).
+constexpr int kDetailTile = 30;
+__global__ void k_detail_map(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_h(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_v(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_radial(LGCR_STAGE_ARGS);

@@ -214,6 +214,170 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     J.detailTmp[o] = ldf(J.Y + o) - r;
 }
 
+// ---------------------------------------------------------------------------
+// Fused detail map (separable kernels, supports up to 8 taps): the horizontal
+// pass of the degraded luma into shared memory, the vertical pass and
+// detail = Y - plain(D(Y)), then the Nyquist passes (at most one per axis:
+// chroma ratios are at most 2) on a 32 x 32 tile with a one-sample halo; the
+// block writes the 30 x 30 interior to the detail plane. Tile samples sit at
+// clamped coordinates, so at the plane borders the halo holds exactly the
+// clamped neighbours the reference's passes read (buildDetailMap,
+// src/algos.cpp:1528-1585, with suppressSourceNyquist 1303-1364).
+// ---------------------------------------------------------------------------
+struct DetailRows {
+    double w[32][8];
+    int ty0[32], r[32];
+    uint32_t act[32];
+    float wsum[32], wabs[32], pos[32];
+};
+
+__device__ __forceinline__ uint32_t activityBits(const uint8_t *am, int n) {
+    uint32_t m = 0;
+    for (int i = 0; i < n; ++i)
+        m |= (__ldg(am + i) != 0 ? 1u : 0u) << i;
+    return m;
+}
+
+template <bool NOCLAMP>
+__device__ __forceinline__ void detailEntry(const float *row, int cw, int tx0, const double (&w)[8],
+                                            uint32_t act, double &hOut, float2 &ext) {
+    double acc = 0.0;
+    float lo = 1e30f, hi = -1e30f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!((act >> i) & 1u))
+            continue;
+        const float a = ldf(row + (NOCLAMP ? tx0 + i : iclamp(tx0 + i, 0, cw - 1)));
+        acc = fma(w[i], (double)a, acc);
+        lo = smin(lo, a);
+        hi = smax(hi, a);
+    }
+    hOut = (double)(float)acc;
+    ext = make_float2(lo, hi);
+}
+
+template <bool NOCLAMP>
+__device__ __forceinline__ double detailVertical(const DetailRows &R, const double (*sH)[32],
+                                                 const float2 (*sE)[32], int k, int lx, int syLo,
+                                                 int ch, float &mn, float &mx) {
+    const int ty0 = R.ty0[k];
+    const uint32_t act = R.act[k];
+    double v = 0.0;
+    float lo = 1e30f, hi = -1e30f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (!((act >> j) & 1u))
+            continue;
+        const int r = (NOCLAMP ? ty0 + j : iclamp(ty0 + j, 0, ch - 1)) - syLo;
+        v = fma(R.w[k][j], sH[r][lx], v);
+        const float2 e = sE[r][lx];
+        lo = smin(lo, e.x);
+        hi = smax(hi, e.y);
+    }
+    mn = lo;
+    mx = hi;
+    return v;
+}
+
+__global__ void __launch_bounds__(256)
+k_detail_map(LGCR_STAGE_ARGS) {
+    __shared__ double sH[kPlainStagedRows][32];
+    __shared__ float2 sE[kPlainStagedRows][32];
+    __shared__ float sD[32][33];
+    __shared__ float sX[32][33];
+    __shared__ DetailRows R;
+    __shared__ FrameJob sJob;
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
+    const int tile = blockIdx.x - tileStart[f];
+    const int w = J.sw, h = J.sh, cw = J.cw, ch = J.ch;
+    const int tilesX = (w + kDetailTile - 1) / kDetailTile;
+    const int x0 = (tile % tilesX) * kDetailTile, y0 = (tile / tilesX) * kDetailTile;
+    const int lx = threadIdx.x, tid = threadIdx.y * 32 + lx;
+    const int c = iclamp(x0 - 1 + lx, 0, w - 1);
+    const AxisView &ax = J.sax, &ay = J.say;
+    const int supY = ay.sup;
+    for (int i = tid; i < 32 * supY; i += 256) {
+        const int k = i / supY, j = i - k * supY;
+        const int rk = iclamp(y0 - 1 + k, 0, h - 1);
+        R.w[k][j] = __ldg(ay.wd + (size_t)rk * supY + j);
+    }
+    if (tid < 32) {
+        const int rk = iclamp(y0 - 1 + tid, 0, h - 1);
+        R.r[tid] = rk;
+        R.ty0[tid] = __ldg(ay.start + rk);
+        R.act[tid] = activityBits(ay.am + (size_t)rk * supY, supY);
+        R.wsum[tid] = __ldg(ay.wsum + rk);
+        R.wabs[tid] = __ldg(ay.wabs + rk);
+        R.pos[tid] = __ldg(ay.pos + rk);
+    }
+    const int syLo = iclamp(__ldg(ay.start + iclamp(y0 - 1, 0, h - 1)), 0, ch - 1);
+    const int syHi = iclamp(__ldg(ay.start + iclamp(y0 + kDetailTile, 0, h - 1)) + supY - 1, 0, ch - 1);
+    const int nRows = syHi - syLo + 1;
+    const float *dgl = J.aff + 8 * (size_t)cw * ch;
+    {
+        // horizontal entries of column c on the chroma rows the tile reads
+        const int supX = ax.sup;
+        const int tx0 = __ldg(ax.start + c);
+        const uint32_t act = activityBits(ax.am + (size_t)c * supX, supX);
+        double wx[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            wx[i] = i < supX ? __ldg(ax.wd + (size_t)c * supX + i) : 0.0;
+        for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
+            const float *row = dgl + (size_t)(syLo + r) * cw;
+            double hv;
+            float2 e;
+            if (J.sNoClampX)
+                detailEntry<true>(row, cw, tx0, wx, act, hv, e);
+            else
+                detailEntry<false>(row, cw, tx0, wx, act, hv, e);
+            sH[r][lx] = hv;
+            sE[r][lx] = e;
+        }
+    }
+    __syncthreads();
+    {
+        const float wsX = __ldg(ax.wsum + c), waX = __ldg(ax.wabs + c), posX = __ldg(ax.pos + c);
+        for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+            float mn, mx;
+            double v = J.sNoClampY ? detailVertical<true>(R, sH, sE, k, lx, syLo, ch, mn, mx)
+                                   : detailVertical<false>(R, sH, sE, k, lx, syLo, ch, mn, mx);
+            const double ws = (double)wsX * (double)R.wsum[k];
+            const double wa = (double)waX * (double)R.wabs[k];
+            if (ws > 1e-6 && ws >= 0.05 * wa)
+                v /= ws;
+            else
+                v = bilinearAt(dgl, cw, ch, posX, R.pos[k]);
+            if (J.clampHull)
+                v = sclamp(v, (double)(mn - J.margin), (double)(mx + J.margin));
+            sD[k][lx] = ldf(J.Y + (size_t)R.r[k] * w + c) - (float)v;
+        }
+    }
+    __syncthreads();
+    const float (*src)[33] = sD;
+    if (J.nyqX) {
+        if (lx >= 1 && lx <= kDetailTile)
+            for (int k = threadIdx.y; k < 32; k += blockDim.y)
+                sX[k][lx] = 0.25f * sD[k][lx - 1] + 0.5f * sD[k][lx] + 0.25f * sD[k][lx + 1];
+        __syncthreads();
+        src = sX;
+    }
+    const int x = x0 - 1 + lx;
+    if (lx < 1 || lx > kDetailTile || x >= w)
+        return;
+    float *dst = const_cast<float *>(J.detailSrc);
+    for (int k = 1 + threadIdx.y; k <= kDetailTile; k += blockDim.y) {
+        const int y = y0 - 1 + k;
+        if (y >= h)
+            break;
+        const float val = J.nyqY ? 0.25f * src[k - 1][lx] + 0.5f * src[k][lx] + 0.25f * src[k + 1][lx]
+                                 : src[k][lx];
+        dst[(size_t)y * w + x] = val;
+    }
+}
+
 // One dyadic pass: x passes (steps 1,2,4..) then y passes; ping-pong
 // between detailTmp and detailTmp2.
 __global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass) {

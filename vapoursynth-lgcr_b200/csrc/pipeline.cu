@@ -320,6 +320,14 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         const ChromaAxis say = buildChromaAxis(sh, sh, rh, shiftY, p.k);
         osax = packAxis(pk, sax);
         osay = packAxis(pk, say);
+        t->sAxSup = sax.sup;
+        t->sAySup = say.sup;
+        for (int y0 = 0; y0 < sh; y0 += kDetailTile) {
+            const int r0 = std::clamp(y0 - 1, 0, sh - 1), r1 = std::clamp(y0 + kDetailTile, 0, sh - 1);
+            const int lo = std::clamp(say.start[r0], 0, ch - 1);
+            const int hi = std::clamp(say.start[r1] + say.sup - 1, 0, ch - 1);
+            t->detailMaxRows = std::max(t->detailMaxRows, hi - lo + 1);
+        }
         if (p.k.radial)
             osrad = packRadial(pk, buildRadialTable(p.k, sax, say, cw, ch));
     }
@@ -651,6 +659,12 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         const float *last = ((J.nyqX + J.nyqY) & 1) ? ws.detailTmp2 : ws.detailTmp;
         J.detailSrc = last;
         J.detail = J.sameSize ? const_cast<float *>(last) : ws.detail;
+        const int nx = (F.sw + int(J.rw) - 1) / int(J.rw);
+        const int ny = (F.sh + int(J.rh) - 1) / int(J.rh);
+        J.sNoClampX = (nx == F.cw && F.cw >= T.sAxSup) ? 1 : 0;
+        J.sNoClampY = (ny == F.ch && F.ch >= T.sAySup) ? 1 : 0;
+        J.detailFused = (J.dTab && !J.radial && J.kernel != 0 && T.sAxSup <= 8 && T.sAySup <= 8 &&
+                         T.detailMaxRows <= kPlainStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
     }
     // algo 4
     J.lgf = ws.lgf;
@@ -673,7 +687,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
 enum StageId : int {
     S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_DIL_H, S_DIL_V,
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
-    S_YC, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
+    S_YC, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
     S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
@@ -687,7 +701,7 @@ const char *stageName(int s) {
         "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
         "buildGuideMaps_tensor", "buildTrustMask_h", "buildTrustMask_v",
         "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
-        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain",
+        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain", "buildDetailMap",
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
         "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
         "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
@@ -768,7 +782,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     const bool resize = !J.sameSize;
     if (s >= S_NYQ0 && s <= S_NYQ7) {
         const int pass = s - S_NYQ0;
-        return (J.guided && J.algo == 6 && pass < J.nyqX + J.nyqY) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
+        return (J.guided && J.algo == 6 && !J.detailFused && pass < J.nyqX + J.nyqY) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
     }
     switch (s) {
     case S_CONVERT: return convertBlocks(J.sw, J.sh) + convertBlocks(J.cw, J.ch);
@@ -787,8 +801,9 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC:
     case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
-    case S_DET_PLAIN: return (J.guided && J.algo == 6) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
+    case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
+    case S_DET_PLAIN: return (J.guided && J.algo == 6 && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
+    case S_DET_MAP: return (J.guided && J.algo == 6 && J.detailFused) ? cdiv(J.sw, kDetailTile) * cdiv(J.sh, kDetailTile) : 0;
     case S_DET_RH: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_RV: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_DET_RR: return (J.guided && J.algo == 6 && resize && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
@@ -874,6 +889,7 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_AFFINE, k_affine, b32x8);
     go(S_DET_HPASS, k_detail_hpass, b32x8);
     go(S_DET_PLAIN, k_detail_plain, b32x8);
+    go(S_DET_MAP, k_detail_map, b32x8);
     for (int pass = 0; pass < 8; ++pass) {
         const int s = S_NYQ0 + pass;
         if (plan.totals[s] == 0)

@@ -122,6 +122,8 @@ struct __align__(16) FrameJob {
     WeightView ycH1, ycV1, ycH2, ycV2; // candidate degradation tables
     WeightView detH, detV;             // detail resample to output (resize)
     int nyqX, nyqY;                    // dyadic Nyquist passes per axis
+    int detailFused;                   // k_detail_map builds the detail map in one pass
+    int sNoClampX, sNoClampY;          // source-grid axes: every chroma tap index in range
     AxisView sax, say;                 // source-grid plain axes (detail map)
     RadialView srad;
     const float *detailSrc;            // Nyquist-filtered detail on the source grid
