@@ -167,6 +167,10 @@ __device__ __forceinline__ float ldf(const float *p) { return __ldg(p); }
 // infinite or NaN arguments take the IEEE division.
 constexpr float kRcpFastLimit = 18446744073709551616.0f;   // 2^64
 
+// The IEEE quotient for the rare arguments outside the fast range, kept out
+// of line so the unrolled tap loops that call rcpAtLeastOne stay compact.
+static __device__ __noinline__ float rcpOutOfRange(float x) { return 1.0f / x; }
+
 __device__ __forceinline__ float rcpAtLeastOne(float x) {
     if (x < kRcpFastLimit) {
         float y;
@@ -174,7 +178,7 @@ __device__ __forceinline__ float rcpAtLeastOne(float x) {
         const float e = __fmaf_rn(-x, y, 1.0f);
         return __fmaf_rn(y, e, y);
     }
-    return 1.0f / x;
+    return rcpOutOfRange(x);
 }
 
 // Dilated trust mask bit of luma sample (x, y).
