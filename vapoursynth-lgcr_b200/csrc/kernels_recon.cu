@@ -513,15 +513,19 @@ struct Acc { double u, v, wsum, sumAbs; };
 
 // One tap of pass 2 (recon.cpp:606-623). dxnx = dx*nx and dxny = (-dx)*ny
 // are the per-column products of the reference's dp and dt, hoisted out of
-// the row loop (same operands, same rounding).
+// the row loop (same operands, same rounding). CHECKED = false when the
+// caller has shown both denominators stay below 2^64 (see guidedPixel).
+template <bool CHECKED>
 __device__ __forceinline__ void tapCore(const TapCtx &c, float l, double2 p, float dxnx, float dxny,
                                         float dy_ny, float dy_nx, float wx, Acc &a) {
     const float dL = l - c.L0;
     const float dp = dxnx + dy_ny;
     const float dt = dxny + dy_nx;
-    const float simRaw = rcpAtLeastOne(1.0f + dL * dL * c.invSigma2);
+    const float xs = 1.0f + dL * dL * c.invSigma2;
+    const float simRaw = CHECKED ? rcpAtLeastOne(xs) : rcpInRange(xs);
     const float sim = 1.0f - c.guideFade * (1.0f - simRaw);
-    const float bump = rcpAtLeastOne(1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par);
+    const float xb = 1.0f + dp * dp * c.invG2 + dt * dt * c.invG2Par;
+    const float bump = CHECKED ? rcpAtLeastOne(xb) : rcpInRange(xb);
     const float w = sim * (wx + c.rescue * bump);
     const double wd = (double)w;
     a.u = fma(wd, p.x, a.u);
@@ -533,7 +537,7 @@ __device__ __forceinline__ void tapCore(const TapCtx &c, float l, double2 p, flo
 __device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float dy_ny, float dy_nx,
                                     float wx, Acc &a) {
     const float dx = dxf * c.rwF;
-    tapCore(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
+    tapCore<true>(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
 }
 
 // Separable base weights, all taps in range, support SUP (fully unrolled;
@@ -562,7 +566,7 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
         for (int i = 0; i < SUP; ++i) {
             if (!((mx >> i) & 1u))
                 continue;
-            tapCore(c, ldf(lrow + i), __ldg(uvrow + i), dxnx[i], dxny[i], dy_ny, dy_nx, wxv[i] * wy, a);
+            tapCore<false>(c, ldf(lrow + i), __ldg(uvrow + i), dxnx[i], dxny[i], dy_ny, dy_nx, wxv[i] * wy, a);
         }
     }
 }
@@ -812,7 +816,12 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     c.invG2 = J.invGsigma2;
     c.invG2Par = J.invGsigma2 / (aniso * aniso);
     Acc a{0.0, 0.0, 0.0, 0.0};
-    const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup;
+    // The unrolled loops skip the reciprocal's range check: every tap's
+    // similarity denominator 1 + dL^2/sigma^2 is at most the same expression
+    // at the window's luma range maxAbsDL (each rounding step is monotonic),
+    // and the frame's bump denominators are bounded on the host.
+    const bool rcpSafe = J.bumpRcpSafe && (1.0f + maxAbsDL * maxAbsDL * invSigma2) < kRcpFastLimit;
+    const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
     if (fast && ax.sup == 8)
         tapsSeparable<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
     else if (fast && ax.sup == 6)

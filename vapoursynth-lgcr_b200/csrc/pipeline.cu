@@ -637,6 +637,14 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.hTab = ws.hTab;
     J.actList = ws.actList;
     J.listed = J.guided && (p.algo == 2 || p.algo == 4);
+    {
+        // guided bump denominator 1 + dp^2/g^2 + dt^2/(g*aniso)^2 with aniso >= 1:
+        // |dp|, |dt| <= (tap distance in chroma samples) * ratio * |n| summed
+        // over both axes; bound it with margin well below 2^64
+        const double d = double(std::max(T.axSup, T.aySup) + 2) * std::max(J.rw, J.rh) * 2.0 * 1.01;
+        const double bound = 1.0 + 2.0 * d * d * double(J.invGsigma2);
+        J.bumpRcpSafe = bound < 1.0e18 ? 1 : 0;
+    }
     J.plainFused = (J.hTab && !J.radial && T.plainMaxRows <= kPlainStagedRows) ? 1 : 0;
     {
         // every tap index in range: starts lie in [0, srcChromaN - sup] and the

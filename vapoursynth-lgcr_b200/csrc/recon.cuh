@@ -110,6 +110,7 @@ struct __align__(16) FrameJob {
     double *uvd;                       // cw x ch x 2: (u, v) in FP64
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
+    int bumpRcpSafe;                   // every guided bump denominator stays below 2^64
     int plainFused;                    // k_plain computes its horizontal rows itself
     int noClampX, noClampY;            // every chroma tap index is in range
     // algo 6 / algo 4 / bm workspaces
@@ -171,13 +172,18 @@ constexpr float kRcpFastLimit = 18446744073709551616.0f;   // 2^64
 // of line so the unrolled tap loops that call rcpAtLeastOne stay compact.
 static __device__ __noinline__ float rcpOutOfRange(float x) { return 1.0f / x; }
 
+// The refinement alone, for callers that have shown x < 2^64 (or NaN, which
+// it returns as the division would).
+__device__ __forceinline__ float rcpInRange(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    const float e = __fmaf_rn(-x, y, 1.0f);
+    return __fmaf_rn(y, e, y);
+}
+
 __device__ __forceinline__ float rcpAtLeastOne(float x) {
-    if (x < kRcpFastLimit) {
-        float y;
-        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-        const float e = __fmaf_rn(-x, y, 1.0f);
-        return __fmaf_rn(y, e, y);
-    }
+    if (x < kRcpFastLimit)
+        return rcpInRange(x);
     return rcpOutOfRange(x);
 }
 
