@@ -30,6 +30,15 @@ cudaStream_t threadStream() {
     return s;
 }
 
+// Plane copy between host and device: one linear copy when both sides are
+// packed (pitch == row bytes), else a 2D copy.
+cudaError_t copyPlane(void *dst, size_t dpitch, const void *src, size_t spitch, size_t rowBytes,
+                      size_t rows, cudaMemcpyKind kind, cudaStream_t s) {
+    if (dpitch == rowBytes && spitch == rowBytes)
+        return cudaMemcpyAsync(dst, src, rowBytes * rows, kind, s);
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, rowBytes, rows, kind, s);
+}
+
 bool checkPlane(const lgcr_plane &p, int w, int h, int bps, bool allowNull) {
     if (!p.data)
         return allowNull;
@@ -137,8 +146,8 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
     cudaError_t e = cudaSuccess;
     if (memory == LGCR_MEM_HOST) {
         for (int i = 0; i < 3; ++i) {
-            e = cudaMemcpy2DAsync(ws->stageIn[i], ws->stageInPitch[i], in[i].data, in[i].stride,
-                                  size_t(in[i].width) * bps, in[i].height, cudaMemcpyHostToDevice, s);
+            e = copyPlane(ws->stageIn[i], ws->stageInPitch[i], in[i].data, in[i].stride,
+                          size_t(in[i].width) * bps, in[i].height, cudaMemcpyHostToDevice, s);
             if (e != cudaSuccess) break;
             t.in[i] = { ws->stageIn[i], (ptrdiff_t)ws->stageInPitch[i], in[i].width, in[i].height };
             t.out[i] = { ws->stageOut[i], (ptrdiff_t)ws->stageOutPitch[i], F.p.outW, F.p.outH };
@@ -166,8 +175,8 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
             if (!out[i].data)
                 continue;
-            e = cudaMemcpy2DAsync(out[i].data, out[i].stride, ws->stageOut[i], ws->stageOutPitch[i],
-                                  size_t(F.p.outW) * bps, F.p.outH, cudaMemcpyDeviceToHost, s);
+            e = copyPlane(out[i].data, out[i].stride, ws->stageOut[i], ws->stageOutPitch[i],
+                          size_t(F.p.outW) * bps, F.p.outH, cudaMemcpyDeviceToHost, s);
         }
     }
     unsigned long long counters[kCntCount] = {};
