@@ -54,6 +54,11 @@ __global__ void k_luma_radial(LGCR_STAGE_ARGS);
 __global__ void k_store_chroma(LGCR_STAGE_ARGS);
 // algo 6
 __global__ void k_yc_h(LGCR_STAGE_ARGS);
+// k_yc_tiled: chroma samples per block side and the most luma rows one
+// block reads per candidate.
+constexpr int kYcTile = 32;
+constexpr int kYcRows = 80;
+__global__ void k_yc_tiled(LGCR_STAGE_ARGS);
 __global__ void k_affine(LGCR_STAGE_ARGS);
 __global__ void k_detail_hpass(LGCR_STAGE_ARGS);
 __global__ void k_detail_plain(LGCR_STAGE_ARGS);

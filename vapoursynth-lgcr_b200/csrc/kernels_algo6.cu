@@ -58,6 +58,80 @@ __global__ void k_yc_h(LGCR_STAGE_ARGS) {
     J.aff[8 * C + o] = median3f(ldf(J.lc + o), y1, y2);   // degraded luma consensus
 }
 
+// The same candidates for a 32 x 32 tile of chroma samples: the horizontal
+// sums of every luma row the tile reads go to shared memory once (per
+// candidate), then each sample runs its vertical pass from there. Same
+// operands and order as candidateAt. Tap supports up to 8.
+__device__ __forceinline__ float ycHorizontal(const FrameJob &J, const WeightView &th, int cx, int row,
+                                              const double (&w)[8], int s0) {
+    const float *lrow = J.Y + (size_t)row * J.sw;
+    double hv = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < th.sup)
+            hv = fma(w[i], (double)ldf(lrow + iclamp(s0 + i, 0, J.sw - 1)), hv);
+    return (float)hv;
+}
+
+__device__ __forceinline__ float ycVertical(const FrameJob &J, const WeightView &tv, int cy,
+                                            const float (*sH)[32], int lo, int lx) {
+    const int sv = __ldg(tv.start + cy);
+    const float *wv = tv.w + (size_t)cy * tv.sup;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (j < tv.sup)
+            acc = fma((double)__ldg(wv + j), (double)sH[iclamp(sv + j, 0, J.sh - 1) - lo][lx], acc);
+    return (float)acc;
+}
+
+__global__ void __launch_bounds__(256)
+k_yc_tiled(LGCR_STAGE_ARGS) {
+    __shared__ float sH1[kYcRows][32];
+    __shared__ float sH2[kYcRows][32];
+    __shared__ FrameJob sJob;
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
+    const int tile = blockIdx.x - tileStart[f];
+    const int tilesX = (J.cw + kYcTile - 1) / kYcTile;
+    const int cx0 = (tile % tilesX) * kYcTile, cy0 = (tile / tilesX) * kYcTile;
+    const int cyLast = min(cy0 + kYcTile, J.ch) - 1;
+    const int lx = threadIdx.x;
+    const int cx = cx0 + lx;
+    const int cxc = min(cx, J.cw - 1);
+    const int lo1 = iclamp(__ldg(J.ycV1.start + cy0), 0, J.sh - 1);
+    const int hi1 = iclamp(__ldg(J.ycV1.start + cyLast) + J.ycV1.sup - 1, 0, J.sh - 1);
+    const int lo2 = iclamp(__ldg(J.ycV2.start + cy0), 0, J.sh - 1);
+    const int hi2 = iclamp(__ldg(J.ycV2.start + cyLast) + J.ycV2.sup - 1, 0, J.sh - 1);
+    {
+        double w1[8], w2[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            w1[i] = i < J.ycH1.sup ? (double)__ldg(J.ycH1.w + (size_t)cxc * J.ycH1.sup + i) : 0.0;
+            w2[i] = i < J.ycH2.sup ? (double)__ldg(J.ycH2.w + (size_t)cxc * J.ycH2.sup + i) : 0.0;
+        }
+        const int s1 = __ldg(J.ycH1.start + cxc), s2 = __ldg(J.ycH2.start + cxc);
+        for (int r = threadIdx.y; r <= hi1 - lo1; r += blockDim.y)
+            sH1[r][lx] = ycHorizontal(J, J.ycH1, cxc, lo1 + r, w1, s1);
+        for (int r = threadIdx.y; r <= hi2 - lo2; r += blockDim.y)
+            sH2[r][lx] = ycHorizontal(J, J.ycH2, cxc, lo2 + r, w2, s2);
+    }
+    __syncthreads();
+    if (cx >= J.cw)
+        return;
+    const size_t C = (size_t)J.cw * J.ch;
+    for (int k = threadIdx.y; cy0 + k <= cyLast; k += blockDim.y) {
+        const int cy = cy0 + k;
+        const size_t o = (size_t)cy * J.cw + cx;
+        const float y1 = ycVertical(J, J.ycV1, cy, sH1, lo1, lx);
+        const float y2 = ycVertical(J, J.ycV2, cy, sH2, lo2, lx);
+        J.yc1[o] = y1;
+        J.yc2[o] = y2;
+        J.aff[8 * C + o] = median3f(ldf(J.lc + o), y1, y2);   // degraded luma consensus
+    }
+}
+
 // 5x5 affine statistics per chroma sample (active samples when sparse).
 __global__ void __launch_bounds__(256)
 k_affine(LGCR_STAGE_ARGS) {
@@ -528,8 +602,13 @@ __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
         ou = sclamp(ou, loU, hiU);
         ov = sclamp(ov, loV, hiV);
     }
-    J.oU[o] = ou;
-    J.oV[o] = ov;
+    if (J.finalInTransfer) {
+        storeChroma(J, 1, ox, oy, ou);
+        storeChroma(J, 2, ox, oy, ov);
+    } else {
+        J.oU[o] = ou;
+        J.oV[o] = ov;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -427,7 +427,9 @@ k_plain(LGCR_STAGE_ARGS) {
             R.pos[tid] = __ldg(J.ay.pos + oy);
         }
     }
-    const bool maskWords = skipListed && J.sparse && J.sameSize;
+    // active-pixel bits: listed pixels are skipped here; algo 6 pixels the
+    // detail transfer leaves alone are stored final here
+    const bool maskWords = (skipListed || J.finalInTransfer) && J.sparse && J.sameSize;
     if (maskWords && tid < rowsHere)
         R.maskWord[tid] = __ldg(J.mask + (size_t)(oy0 + tid) * J.maskWords + (colBase >> 5));
     if (fused) {
@@ -464,9 +466,10 @@ k_plain(LGCR_STAGE_ARGS) {
     for (int k = threadIdx.y; k < rowsHere; k += blockDim.y) {
         const int oy = oy0 + k;
         // listed pixels of algo 2 and integer algo 4 are written by k_guided
-        if (skipListed) {
-            const bool act = maskWords ? ((R.maskWord[k] >> lx) & 1u) != 0 : pixelActive(J, ox, oy);
-            if (act)
+        bool act = false;
+        if (skipListed || J.finalInTransfer) {
+            act = maskWords ? ((R.maskWord[k] >> lx) & 1u) != 0 : pixelActive(J, ox, oy);
+            if (act && skipListed)
                 continue;
         }
         float u, v;
@@ -489,10 +492,15 @@ k_plain(LGCR_STAGE_ARGS) {
         } else {
             plainPixel(J, ox, oy, u, v);
         }
-        if (floatSelector) {
+        if (floatSelector || (J.finalInTransfer && act)) {
             const size_t o = (size_t)oy * J.W + ox;
-            J.oU[o] = u;                    // base for the selector blend
+            J.oU[o] = u;                    // base for the selector blend / detail transfer
             J.oV[o] = v;
+            continue;
+        }
+        if (J.finalInTransfer) {
+            storeChroma(J, 1, ox, oy, u);
+            storeChroma(J, 2, ox, oy, v);
             continue;
         }
         emit(J, ox, oy, u, v);

@@ -312,10 +312,21 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         bil.kernel = Kernel::Bilinear; bil.kp1 = bil.kp2 = 0.0; bil.support = 1.0;
         KernelSpec bic;
         bic.kernel = Kernel::Bicubic; bic.kp1 = 0.0; bic.kp2 = 0.6; bic.support = 2.0;
-        oy1h = packWeights(pk, buildWeights(sw, cw, bil, shiftX));
-        oy1v = packWeights(pk, buildWeights(sh, ch, bil, shiftY));
-        oy2h = packWeights(pk, buildWeights(sw, cw, bic, shiftX));
-        oy2v = packWeights(pk, buildWeights(sh, ch, bic, shiftY));
+        const WeightTable y1h = buildWeights(sw, cw, bil, shiftX), y1v = buildWeights(sh, ch, bil, shiftY);
+        const WeightTable y2h = buildWeights(sw, cw, bic, shiftX), y2v = buildWeights(sh, ch, bic, shiftY);
+        oy1h = packWeights(pk, y1h);
+        oy1v = packWeights(pk, y1v);
+        oy2h = packWeights(pk, y2h);
+        oy2v = packWeights(pk, y2v);
+        t->ycMaxSup = std::max(std::max(y1h.sup, y1v.sup), std::max(y2h.sup, y2v.sup));
+        for (int c0 = 0; c0 < ch; c0 += kYcTile) {
+            const int c1 = std::min(c0 + kYcTile, ch) - 1;
+            for (const WeightTable *v : {&y1v, &y2v}) {
+                const int lo = std::clamp(v->start[c0], 0, sh - 1);
+                const int hi = std::clamp(v->start[c1] + v->sup - 1, 0, sh - 1);
+                t->ycMaxRows = std::max(t->ycMaxRows, hi - lo + 1);
+            }
+        }
         const ChromaAxis sax = buildChromaAxis(sw, sw, rw, shiftX, p.k);
         const ChromaAxis say = buildChromaAxis(sh, sh, rh, shiftY, p.k);
         osax = packAxis(pk, sax);
@@ -671,6 +682,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         const int ny = (F.sh + int(J.rh) - 1) / int(J.rh);
         J.sNoClampX = (nx == F.cw && F.cw >= T.sAxSup) ? 1 : 0;
         J.sNoClampY = (ny == F.ch && F.ch >= T.sAySup) ? 1 : 0;
+        J.ycTiled = (T.ycMaxSup <= 8 && T.ycMaxRows <= kYcRows) ? 1 : 0;
         J.detailFused = (J.dTab && !J.radial && J.kernel != 0 && T.sAxSup <= 8 && T.sAySup <= 8 &&
                          T.detailMaxRows <= kPlainStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
     }
@@ -687,6 +699,9 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.bmSigma = float(p.sigma);
     if (!T.bmStartsX)
         J.bm = 0;                                 // frame smaller than one patch
+    // algo 6 with nothing after the detail transfer: the plain stage stores
+    // the pixels the transfer leaves alone, the transfer stores the others
+    J.finalInTransfer = (p.algo == 6 && J.guided && !J.bm && !J.needBackProject) ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -695,7 +710,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
 enum StageId : int {
     S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_DIL_H, S_DIL_V,
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
-    S_YC, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
+    S_YC, S_YC_TILED, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
     S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
@@ -709,7 +724,7 @@ const char *stageName(int s) {
         "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
         "buildGuideMaps_tensor", "buildTrustMask_h", "buildTrustMask_v",
         "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
-        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain", "buildDetailMap",
+        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps_candidates_tiled", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain", "buildDetailMap",
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
         "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
         "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
@@ -807,7 +822,8 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_HPASS: return (J.hTab && !J.radial && !J.plainFused && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
     case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, kPlainRows);
     case S_GUIDED: return J.listed ? 1 : 0;
-    case S_YC:
+    case S_YC: return (J.guided && J.algo == 6 && !J.ycTiled) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_YC_TILED: return (J.guided && J.algo == 6 && J.ycTiled) ? cdiv(J.cw, kYcTile) * cdiv(J.ch, kYcTile) : 0;
     case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_PLAIN: return (J.guided && J.algo == 6 && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
@@ -822,7 +838,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_BM_AGG: return J.bm ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_BP: return J.needBackProject ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_ROI: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_STORE: return J.directOutput ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_STORE: return (J.directOutput || J.finalInTransfer) ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
     }
     return 0;
 }
@@ -894,6 +910,7 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
         ++launches;
     }
     go(S_YC, k_yc_h, b32x8);
+    go(S_YC_TILED, k_yc_tiled, b32x8);
     go(S_AFFINE, k_affine, b32x8);
     go(S_DET_HPASS, k_detail_hpass, b32x8);
     go(S_DET_PLAIN, k_detail_plain, b32x8);

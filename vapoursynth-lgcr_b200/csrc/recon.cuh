@@ -79,6 +79,8 @@ struct __align__(16) FrameJob {
     int guided;                        // strength > 0
     int useMs, clampHull, trustOn, dil;
     int directOutput;                  // recon kernel quantizes and stores
+    int finalInTransfer;               // algo 6: plain (inactive) and detail transfer
+                                       // (active pixels) quantize and store
     int needBackProject;
     float strength, sigma, sratio, sdb, stretch, invGsigma2, rescue;
     float strength4;                   // algo 4 selector strength (lambda)
@@ -124,6 +126,7 @@ struct __align__(16) FrameJob {
     WeightView detH, detV;             // detail resample to output (resize)
     int nyqX, nyqY;                    // dyadic Nyquist passes per axis
     int detailFused;                   // k_detail_map builds the detail map in one pass
+    int ycTiled;                       // k_yc_tiled builds the degradation candidates
     int sNoClampX, sNoClampY;          // source-grid axes: every chroma tap index in range
     AxisView sax, say;                 // source-grid plain axes (detail map)
     RadialView srad;
