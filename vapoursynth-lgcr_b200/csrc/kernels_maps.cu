@@ -22,25 +22,88 @@ namespace lgcr_b200 {
 // it to a same-size output), the rest the chroma planes; the chroma blocks
 // also clear the chroma work masks and compute lc from the luma codes.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t rawAt(const void *plane, long long pitch, int kind, int x, int y) {
-    const char *row = static_cast<const char *>(plane) + (long long)y * pitch;
-    if (kind == kU16)
+// Sample access specialised on the sample type (row pointers hoisted).
+template <int KIND>
+__device__ __forceinline__ uint32_t rawLoad(const char *row, int x) {
+    if (KIND == kU16)
         return __ldg(reinterpret_cast<const unsigned short *>(row) + x);
-    if (kind == kU8)
+    if (KIND == kU8)
         return __ldg(reinterpret_cast<const unsigned char *>(row) + x);
     return __float_as_uint(__ldg(reinterpret_cast<const float *>(row) + x));
 }
 
-// planeToFloat of one sample: s * scale + offset in double, then float.
-__device__ __forceinline__ float toFloat(const FrameJob &J, uint32_t raw, double off) {
-    return J.inKind == kF32 ? __uint_as_float(raw) : (float)((double)raw * J.yScale + off);
+template <int KIND>
+__device__ __forceinline__ void rawStore(char *row, int x, uint32_t raw) {
+    if (KIND == kU16) reinterpret_cast<unsigned short *>(row)[x] = (unsigned short)raw;
+    else if (KIND == kU8) reinterpret_cast<unsigned char *>(row)[x] = (unsigned char)raw;
+    else reinterpret_cast<uint32_t *>(row)[x] = raw;
 }
 
-__device__ __forceinline__ void storeRaw(void *plane, long long pitch, int kind, int x, int y, uint32_t raw) {
-    char *row = static_cast<char *>(plane) + (long long)y * pitch;
-    if (kind == kU16) reinterpret_cast<unsigned short *>(row)[x] = (unsigned short)raw;
-    else if (kind == kU8) reinterpret_cast<unsigned char *>(row)[x] = (unsigned char)raw;
-    else reinterpret_cast<uint32_t *>(row)[x] = raw;
+// planeToFloat of one sample: s * scale + offset in double, then float.
+template <int KIND>
+__device__ __forceinline__ float rawToFloat(uint32_t raw, double scale, double off) {
+    return KIND == kF32 ? __uint_as_float(raw) : (float)((double)raw * scale + off);
+}
+
+template <int KIND>
+__device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, int lane) {
+    const char *src = static_cast<const char *>(J.in[0]) + (long long)y * J.inPitch[0];
+    char *dst = (J.writeLuma && J.sameSize) ? static_cast<char *>(J.out[0]) + (long long)y * J.outPitch[0]
+                                            : nullptr;
+    float *yw = J.Yw ? J.Yw + (size_t)y * J.sw : nullptr;
+    const double scale = J.yScale;
+    const int w = J.sw;
+#pragma unroll 4
+    for (int k = 0; k < kConvertSpan / 32; ++k) {
+        const int x = xb + lane + 32 * k;
+        if (x >= w)
+            break;
+        const uint32_t raw = rawLoad<KIND>(src, x);
+        if (yw)
+            yw[x] = rawToFloat<KIND>(raw, scale, 0.0);
+        if (dst)
+            rawStore<KIND>(dst, x, raw);
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void convertChroma(const FrameJob &J, int cy, int xb, int lane) {
+    const char *su = static_cast<const char *>(J.in[1]) + (long long)cy * J.inPitch[1];
+    const char *sv = static_cast<const char *>(J.in[2]) + (long long)cy * J.inPitch[2];
+    const size_t rowOff = (size_t)cy * J.cw;
+    const double scale = J.yScale, off = J.cOffset;
+    int yb = 0, ye = 0;
+    const char *lrow0 = nullptr;
+    const long long lpitch = J.inPitch[0];
+    if (J.lc) {
+        yb = __ldg(J.lcYb + cy);
+        ye = __ldg(J.lcYe + cy);
+        lrow0 = static_cast<const char *>(J.in[0]) + (long long)yb * lpitch;
+    }
+#pragma unroll 2
+    for (int k = 0; k < kConvertSpan / 32; ++k) {
+        const int cx = xb + lane + 32 * k;
+        if (cx >= J.cw)
+            break;
+        const size_t o = rowOff + cx;
+        const float u = rawToFloat<KIND>(rawLoad<KIND>(su, cx), scale, off);
+        const float v = rawToFloat<KIND>(rawLoad<KIND>(sv, cx), scale, off);
+        if (J.Uw) J.Uw[o] = u;
+        if (J.Vw) J.Vw[o] = v;
+        if (J.uvd) reinterpret_cast<double2 *>(J.uvd)[o] = make_double2((double)u, (double)v);
+        if (J.cmask) J.cmask[o] = 0;
+        if (J.roi) J.roi[o] = 0;
+        if (J.lc) {
+            // buildLcMap: raster-order double sum over the footprint
+            const int xb0 = __ldg(J.lcXb + cx), xe0 = __ldg(J.lcXe + cx);
+            double sum = 0.0;
+            const char *lrow = lrow0;
+            for (int j = yb; j < ye; ++j, lrow += lpitch)
+                for (int i = xb0; i < xe0; ++i)
+                    sum += (double)rawToFloat<KIND>(rawLoad<KIND>(lrow, i), scale, 0.0);
+            J.lc[o] = (float)(sum / ((double)(xe0 - xb0) * (double)(ye - yb)));
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kConvertWarps * 32)
@@ -60,17 +123,10 @@ k_convert(LGCR_STAGE_ARGS) {
         if (gw == 0 && lane < kCntCount)
             J.counters[lane] = 0ull;
         const int y = gw / gpr, xb = (gw % gpr) * kConvertSpan;
-        const bool copy = J.writeLuma && J.sameSize;
-#pragma unroll 4
-        for (int k = 0; k < kConvertSpan / 32; ++k) {
-            const int x = xb + lane + 32 * k;
-            if (x >= J.sw)
-                break;
-            const uint32_t raw = rawAt(J.in[0], J.inPitch[0], J.inKind, x, y);
-            if (J.Yw)
-                J.Yw[(size_t)y * J.sw + x] = toFloat(J, raw, 0.0);
-            if (copy)
-                storeRaw(J.out[0], J.outPitch[0], J.inKind, x, y, raw);
+        switch (J.inKind) {
+        case kU8: convertLuma<kU8>(J, y, xb, lane); break;
+        case kU16: convertLuma<kU16>(J, y, xb, lane); break;
+        default: convertLuma<kF32>(J, y, xb, lane); break;
         }
         return;
     }
@@ -79,33 +135,10 @@ k_convert(LGCR_STAGE_ARGS) {
     if (gw >= J.ch * gpr)
         return;
     const int cy = gw / gpr, xb = (gw % gpr) * kConvertSpan;
-    int yb = 0, ye = 0;
-    if (J.lc) {
-        yb = __ldg(J.lcYb + cy);
-        ye = __ldg(J.lcYe + cy);
-    }
-#pragma unroll 2
-    for (int k = 0; k < kConvertSpan / 32; ++k) {
-        const int cx = xb + lane + 32 * k;
-        if (cx >= J.cw)
-            break;
-        const size_t o = (size_t)cy * J.cw + cx;
-        const float u = toFloat(J, rawAt(J.in[1], J.inPitch[1], J.inKind, cx, cy), J.cOffset);
-        const float v = toFloat(J, rawAt(J.in[2], J.inPitch[2], J.inKind, cx, cy), J.cOffset);
-        if (J.Uw) J.Uw[o] = u;
-        if (J.Vw) J.Vw[o] = v;
-        if (J.uvd) reinterpret_cast<double2 *>(J.uvd)[o] = make_double2((double)u, (double)v);
-        if (J.cmask) J.cmask[o] = 0;
-        if (J.roi) J.roi[o] = 0;
-        if (J.lc) {
-            // buildLcMap: raster-order double sum over the footprint
-            const int xb0 = __ldg(J.lcXb + cx), xe0 = __ldg(J.lcXe + cx);
-            double sum = 0.0;
-            for (int j = yb; j < ye; ++j)
-                for (int i = xb0; i < xe0; ++i)
-                    sum += (double)toFloat(J, rawAt(J.in[0], J.inPitch[0], J.inKind, i, j), 0.0);
-            J.lc[o] = (float)(sum / ((double)(xe0 - xb0) * (double)(ye - yb)));
-        }
+    switch (J.inKind) {
+    case kU8: convertChroma<kU8>(J, cy, xb, lane); break;
+    case kU16: convertChroma<kU16>(J, cy, xb, lane); break;
+    default: convertChroma<kF32>(J, cy, xb, lane); break;
     }
 }
 
@@ -438,12 +471,81 @@ k_count(LGCR_STAGE_ARGS) {
 // an active sample can read them.
 // ---------------------------------------------------------------------------
 constexpr int GT_X = 32, GT_Y = 8, GH = 4;
+constexpr int GW = GT_X + 2 * GH, GHh = GT_Y + 2 * GH;
+
+// Gradients of the three planes at one tile slot: (gx, gy) of lc and U in
+// one 16-byte word, of V in an 8-byte word, so a bilinear corner is two
+// shared-memory loads.
+struct GateTile {
+    float4 g01[GHh][GW];
+    float2 g2[GHh][GW];
+};
+
+// Gate of the active sample (x, y). INTERIOR: the tile and its halo lie
+// inside the plane, so sample slots need no clamping.
+template <bool INTERIOR>
+__device__ __forceinline__ float gateAt(const GateTile &T, int x, int y, int x0, int y0, int w, int h) {
+    auto sx = [&](int xx) { return (INTERIOR ? xx : iclamp(xx, 0, w - 1)) - x0 + GH; };
+    auto sy = [&](int yy) { return (INTERIOR ? yy : iclamp(yy, 0, h - 1)) - y0 + GH; };
+    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+            const float4 g = T.g01[sy(y + dy)][sx(x + dx)];
+            const float a = g.x, b = g.y;
+            sxx += a * a; sxy += a * b; syy += b * b;
+        }
+    const float jsum = sxx + syy;
+    if (jsum < 1e-10f)
+        return 0.0f;
+    const TensorDir dir = principalDirection(sxx, sxy, syy);
+    const float nx = dir.nx, ny = dir.ny;
+    float sumY = 0, sqY = 0, momY = 0, sumC = 0, sqC = 0, momC = 0;
+    for (int k = -3; k <= 3; ++k) {
+        const float px = (float)x + (float)k * nx;
+        const float py = (float)y + (float)k * ny;
+        const float fpx = floorf(px), fpy = floorf(py);
+        const int rawX = (int)fpx, rawY = (int)fpy;
+        const int bx0 = sx(rawX), bx1 = sx(rawX + 1);
+        const int by0 = sy(rawY), by1 = sy(rawY + 1);
+        const float fx = px - fpx, fy = py - fpy;
+        const float4 A = T.g01[by0][bx0], B = T.g01[by0][bx1], C = T.g01[by1][bx0], D = T.g01[by1][bx1];
+        const float2 A2 = T.g2[by0][bx0], B2 = T.g2[by0][bx1], C2 = T.g2[by1][bx0], D2 = T.g2[by1][bx1];
+        float s[3];
+        {
+            const float a = A.x * nx + A.y * ny, b = B.x * nx + B.y * ny;
+            const float c = C.x * nx + C.y * ny, d = D.x * nx + D.y * ny;
+            s[0] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+        }
+        {
+            const float a = A.z * nx + A.w * ny, b = B.z * nx + B.w * ny;
+            const float c = C.z * nx + C.w * ny, d = D.z * nx + D.w * ny;
+            s[1] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+        }
+        {
+            const float a = A2.x * nx + A2.y * ny, b = B2.x * nx + B2.y * ny;
+            const float c = C2.x * nx + C2.y * ny, d = D2.x * nx + D2.y * ny;
+            s[2] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+        }
+        const float gY = fabsf(s[0]);
+        const float gC = sqrtf(s[1] * s[1] + s[2] * s[2]);
+        sumY += gY; sqY += gY * gY; momY += (float)k * gY;
+        sumC += gC; sqC += gC * gC; momC += (float)k * gC;
+    }
+    if (sumY < 1e-9f || sumC < 1e-9f)
+        return 0.0f;
+    const float partY = sumY * sumY / (sqY + 1e-12f);
+    const float partC = sumC * sumC / (sqC + 1e-12f);
+    const float ratio = partC / (partY + 1e-6f);
+    const float dcent = fabsf(momY / sumY - momC / sumC);
+    const float tw = sclamp((1.6f - ratio) / 0.4f, 0.0f, 1.0f);
+    const float tp = sclamp((1.0f - dcent) / 0.5f, 0.0f, 1.0f);
+    return (tw * tw * (3.0f - 2.0f * tw)) * (tp * tp * (3.0f - 2.0f * tp));
+}
 
 __global__ void __launch_bounds__(GT_X * GT_Y)
 k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     __shared__ float src[3][GT_Y + 2 * GH + 2][GT_X + 2 * GH + 2];
-    __shared__ float gx[3][GT_Y + 2 * GH][GT_X + 2 * GH];
-    __shared__ float gy[3][GT_Y + 2 * GH][GT_X + 2 * GH];
+    __shared__ GateTile T;
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     stageJob(jobs, f, sJob);
@@ -463,17 +565,24 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
         src[p][r][c] = ldf(planes[p] + (size_t)yy * w + xx);
     }
     __syncthreads();
-    constexpr int GW = GT_X + 2 * GH, GHh = GT_Y + 2 * GH;
-    for (int i = tid; i < 3 * GW * GHh; i += nthreads) {
-        const int p = i / (GW * GHh), rem = i % (GW * GHh);
-        const int r = rem / GW, c = rem % GW;
+    // gradients at clamped positions of the tile and its halo (the dense
+    // Sobel rows of the reference; the sparse reference computes the same
+    // values wherever an active sample reads them)
+    for (int i = tid; i < GW * GHh; i += nthreads) {
+        const int r = i / GW, c = i % GW;
         const int yy = iclamp(y0 - GH + r, 0, h - 1), xx = iclamp(x0 - GH + c, 0, w - 1);
         const int sr = yy - y0 + GH + 1, sc = xx - x0 + GH + 1;
-        const float tl = src[p][sr - 1][sc - 1], t = src[p][sr - 1][sc], tr = src[p][sr - 1][sc + 1];
-        const float l = src[p][sr][sc - 1], rr = src[p][sr][sc + 1];
-        const float bl = src[p][sr + 1][sc - 1], b = src[p][sr + 1][sc], br = src[p][sr + 1][sc + 1];
-        gx[p][r][c] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
-        gy[p][r][c] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
+        float g[6];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+            const float tl = src[p][sr - 1][sc - 1], t = src[p][sr - 1][sc], tr = src[p][sr - 1][sc + 1];
+            const float l = src[p][sr][sc - 1], rr = src[p][sr][sc + 1];
+            const float bl = src[p][sr + 1][sc - 1], b = src[p][sr + 1][sc], br = src[p][sr + 1][sc + 1];
+            g[2 * p] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
+            g[2 * p + 1] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
+        }
+        T.g01[r][c] = make_float4(g[0], g[1], g[2], g[3]);
+        T.g2[r][c] = make_float2(g[4], g[5]);
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
@@ -486,56 +595,8 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
         J.ms[o] = 0.0f;
         return;
     }
-    // slot of a clamped coordinate
-    auto sx = [&](int xx) { return iclamp(xx, 0, w - 1) - x0 + GH; };
-    auto sy = [&](int yy) { return iclamp(yy, 0, h - 1) - y0 + GH; };
-    float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;
-    for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-            const float a = gx[0][sy(y + dy)][sx(x + dx)];
-            const float b = gy[0][sy(y + dy)][sx(x + dx)];
-            sxx += a * a; sxy += a * b; syy += b * b;
-        }
-    const float jsum = sxx + syy;
-    if (jsum < 1e-10f) {
-        J.ms[o] = 0.0f;
-        return;
-    }
-    const TensorDir dir = principalDirection(sxx, sxy, syy);
-    const float nx = dir.nx, ny = dir.ny;
-    float sumY = 0, sqY = 0, momY = 0, sumC = 0, sqC = 0, momC = 0;
-    for (int k = -3; k <= 3; ++k) {
-        const float px = (float)x + (float)k * nx;
-        const float py = (float)y + (float)k * ny;
-        const float fpx = floorf(px), fpy = floorf(py);
-        const int rawX = (int)fpx, rawY = (int)fpy;
-        const int bx0 = sx(rawX), bx1 = sx(rawX + 1);
-        const int by0 = sy(rawY), by1 = sy(rawY + 1);
-        const float fx = px - fpx, fy = py - fpy;
-        float s[3];
-        for (int p = 0; p < 3; ++p) {
-            const float a = gx[p][by0][bx0] * nx + gy[p][by0][bx0] * ny;
-            const float b = gx[p][by0][bx1] * nx + gy[p][by0][bx1] * ny;
-            const float c = gx[p][by1][bx0] * nx + gy[p][by1][bx0] * ny;
-            const float d = gx[p][by1][bx1] * nx + gy[p][by1][bx1] * ny;
-            s[p] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
-        }
-        const float gY = fabsf(s[0]);
-        const float gC = sqrtf(s[1] * s[1] + s[2] * s[2]);
-        sumY += gY; sqY += gY * gY; momY += (float)k * gY;
-        sumC += gC; sqC += gC * gC; momC += (float)k * gC;
-    }
-    if (sumY < 1e-9f || sumC < 1e-9f) {
-        J.ms[o] = 0.0f;
-        return;
-    }
-    const float partY = sumY * sumY / (sqY + 1e-12f);
-    const float partC = sumC * sumC / (sqC + 1e-12f);
-    const float ratio = partC / (partY + 1e-6f);
-    const float dcent = fabsf(momY / sumY - momC / sumC);
-    const float tw = sclamp((1.6f - ratio) / 0.4f, 0.0f, 1.0f);
-    const float tp = sclamp((1.0f - dcent) / 0.5f, 0.0f, 1.0f);
-    J.ms[o] = (tw * tw * (3.0f - 2.0f * tw)) * (tp * tp * (3.0f - 2.0f * tp));
+    const bool interior = x0 >= GH && y0 >= GH && x0 + GT_X + GH <= w && y0 + GT_Y + GH <= h;
+    J.ms[o] = interior ? gateAt<true>(T, x, y, x0, y0, w, h) : gateAt<false>(T, x, y, x0, y0, w, h);
 }
 
 } // namespace lgcr_b200
