@@ -264,6 +264,25 @@ RadialTable buildRadialTable(const KernelSpec &k, const ChromaAxis &ax, const Ch
     return t;
 }
 
+void rescueFactors(const ChromaAxis &a, std::vector<float> &mx, std::vector<float> &ss) {
+    mx.assign(a.n, 0.0f);
+    ss.assign(a.n, 0.0f);
+    if (a.w.empty())
+        return;                                   // radial axes carry no weights
+    for (int i = 0; i < a.n; ++i) {
+        float m = 0.0f, q = 0.0f;
+        for (int j = 0; j < a.sup; ++j) {
+            if (a.am[size_t(i) * a.sup + j] == 0)
+                continue;
+            const float w = a.w[size_t(i) * a.sup + j];
+            m = (m < std::fabs(w)) ? std::fabs(w) : m;
+            q += w * w;
+        }
+        mx[i] = m;
+        ss[i] = q;
+    }
+}
+
 void lcExtents(int lumaN, int chromaN, double r, double shift,
                std::vector<int> &begin, std::vector<int> &end) {
     begin.resize(chromaN);

@@ -74,6 +74,11 @@ struct RadialTable {
 RadialTable buildRadialTable(const KernelSpec &k, const ChromaAxis &ax, const ChromaAxis &ay,
                              int sourceWidth, int sourceHeight);
 
+// Per index of a separable chroma axis: the largest |weight| and the sum of
+// squared weights over the active taps (the guided rescue term's kappa
+// factors), in float and in tap order as the guided pass evaluates them.
+void rescueFactors(const ChromaAxis &a, std::vector<float> &mx, std::vector<float> &ss);
+
 // Footprint extents of each chroma sample on the luma grid.
 void lcExtents(int lumaN, int chromaN, double r, double shift,
                std::vector<int> &begin, std::vector<int> &end);

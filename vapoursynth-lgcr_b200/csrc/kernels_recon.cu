@@ -548,19 +548,80 @@ __device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float 
     tapCore<true>(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
 }
 
-// Separable base weights, all taps in range, support SUP (fully unrolled;
-// the per-column products dx*nx and (-dx)*ny stay in registers).
+// Two taps' FP32 arithmetic per instruction: the packed f32x2 add, sub, mul
+// and fma of sm_100 round each lane exactly like the scalar instruction.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void up2(f32x2 r, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// rcpInRange on both lanes: hardware approximation per lane, then the same
+// fused Newton-Raphson refinement e = 1 - x*y, y' = y + y*e on the pair.
+__device__ __forceinline__ f32x2 rcp2(f32x2 x, f32x2 one) {
+    float x0, x1, y0, y1;
+    up2(x, x0, x1);
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(x0));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(x1));
+    const f32x2 y = pk2(y0, y1);
+    const f32x2 e = fma2(x ^ 0x8000000080000000ull, y, one);     // -x: sign bits flipped
+    return fma2(y, e, y);
+}
+
+__device__ __forceinline__ void accumulate(Acc &a, float w, double2 p) {
+    const double wd = (double)w;
+    a.u = fma(wd, p.x, a.u);
+    a.v = fma(wd, p.y, a.v);
+    a.wsum += wd;
+    a.sumAbs += fabs(wd);
+}
+
+// Separable base weights, all taps in range, support SUP (even; fully
+// unrolled). The per-column products dx*nx and (-dx)*ny stay in registers;
+// columns are processed in pairs with tapCore's arithmetic on packed pairs
+// (range checks of the reciprocals hoisted by the caller), and each active
+// tap is accumulated in FP64 in tap order.
 template <int SUP>
 __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
                                               const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
-    float dxnx[SUP], dxny[SUP], wxv[SUP];
+    constexpr int NP = SUP / 2;
+    f32x2 dxnx[NP], dxny[NP], wxv[NP];
 #pragma unroll
-    for (int i = 0; i < SUP; ++i) {
-        const float dx = ((float)(tx0 + i) - c.scx) * c.rwF;
-        dxnx[i] = dx * c.nx;
-        dxny[i] = -dx * c.ny;
-        wxv[i] = __ldg(wxp + i);
+    for (int q = 0; q < NP; ++q) {
+        const float dx0 = ((float)(tx0 + 2 * q) - c.scx) * c.rwF;
+        const float dx1 = ((float)(tx0 + 2 * q + 1) - c.scx) * c.rwF;
+        dxnx[q] = pk2(dx0 * c.nx, dx1 * c.nx);
+        dxny[q] = pk2(-dx0 * c.ny, -dx1 * c.ny);
+        wxv[q] = pk2(__ldg(wxp + 2 * q), __ldg(wxp + 2 * q + 1));
     }
+    const f32x2 one = pk2(1.0f, 1.0f);
+    const f32x2 L0 = pk2(c.L0, c.L0), invS = pk2(c.invSigma2, c.invSigma2);
+    const f32x2 fade = pk2(c.guideFade, c.guideFade), resc = pk2(c.rescue, c.rescue);
+    const f32x2 g2 = pk2(c.invG2, c.invG2), g2p = pk2(c.invG2Par, c.invG2Par);
 #pragma unroll
     for (int j = 0; j < SUP; ++j) {
         if (!((my >> j) & 1u))
@@ -569,12 +630,25 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
         const double2 *uvrow = c.uv + (size_t)(ty0 + j) * c.cw + tx0;
         const float wy = __ldg(wyp + j);
         const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
-        const float dy_ny = dy * c.ny, dy_nx = dy * c.nx;
+        const f32x2 wyy = pk2(wy, wy);
+        const f32x2 dyny = pk2(dy * c.ny, dy * c.ny), dynx = pk2(dy * c.nx, dy * c.nx);
 #pragma unroll
-        for (int i = 0; i < SUP; ++i) {
-            if (!((mx >> i) & 1u))
-                continue;
-            tapCore<false>(c, ldf(lrow + i), __ldg(uvrow + i), dxnx[i], dxny[i], dy_ny, dy_nx, wxv[i] * wy, a);
+        for (int q = 0; q < NP; ++q) {
+            const int i = 2 * q;
+            const double2 p0 = __ldg(uvrow + i), p1 = __ldg(uvrow + i + 1);
+            const f32x2 dL = sub2(pk2(ldf(lrow + i), ldf(lrow + i + 1)), L0);
+            const f32x2 simRaw = rcp2(add2(one, mul2(mul2(dL, dL), invS)), one);
+            const f32x2 sim = sub2(one, mul2(fade, sub2(one, simRaw)));
+            const f32x2 dp = add2(dxnx[q], dyny);
+            const f32x2 dt = add2(dxny[q], dynx);
+            const f32x2 bump = rcp2(add2(add2(one, mul2(mul2(dp, dp), g2)), mul2(mul2(dt, dt), g2p)), one);
+            const f32x2 w = mul2(sim, add2(mul2(wxv[q], wyy), mul2(resc, bump)));
+            float w0, w1;
+            up2(w, w0, w1);
+            if ((mx >> i) & 1u)
+                accumulate(a, w0, p0);
+            if ((mx >> (i + 1)) & 1u)
+                accumulate(a, w1, p1);
         }
     }
 }
@@ -777,19 +851,10 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
         if (rescue > 0.0f) {
             float kappa;
             if (!J.radial) {
-                float mxX = 0, ssX = 0, mxY = 0, ssY = 0;
-                for (int i = 0; i < ax.sup; ++i)
-                    if (__ldg(amx + i) > 0) {
-                        const float w = __ldg(wxp + i);
-                        mxX = smax(mxX, fabsf(w));
-                        ssX += w * w;
-                    }
-                for (int j = 0; j < ay.sup; ++j)
-                    if (__ldg(amy + j) > 0) {
-                        const float w = __ldg(wyp + j);
-                        mxY = smax(mxY, fabsf(w));
-                        ssY += w * w;
-                    }
+                // per-axis max |w| and sum of w^2 over the active taps (host tables
+                // of the same float sums)
+                const float mxX = __ldg(ax.kmx + ox), ssX = __ldg(ax.kss + ox);
+                const float mxY = __ldg(ay.kmx + oy), ssY = __ldg(ay.kss + oy);
                 kappa = (mxX * mxX * mxY * mxY) / (ssX * ssY + 1e-12f);
             } else {
                 const float *base = radialWeightsAt(J.rad, ox, oy);

@@ -221,7 +221,7 @@ struct Packer {
     }
 };
 
-struct AxisOffsets { size_t start, w, wd, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF; int n, sup; };
+struct AxisOffsets { size_t start, w, wd, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF, kmx, kss; int n, sup; };
 
 AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
     AxisOffsets o;
@@ -232,6 +232,9 @@ AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
     o.pos = pk.add(a.pos); o.lpos = pk.add(a.lpos);
     o.cbI0 = pk.add(a.chromaBilin.i0); o.cbF = pk.add(a.chromaBilin.f);
     o.lbI0 = pk.add(a.lumaBilin.i0); o.lbF = pk.add(a.lumaBilin.f);
+    std::vector<float> kmx, kss;
+    rescueFactors(a, kmx, kss);
+    o.kmx = pk.add(kmx); o.kss = pk.add(kss);
     return o;
 }
 
@@ -245,6 +248,7 @@ AxisView axisView(const DeviceArena &ar, const AxisOffsets &o) {
     v.lpos = (const float *)ar.at(o.lpos); v.cbI0 = (const int *)ar.at(o.cbI0);
     v.cbF = (const float *)ar.at(o.cbF); v.lbI0 = (const int *)ar.at(o.lbI0);
     v.lbF = (const float *)ar.at(o.lbF);
+    v.kmx = (const float *)ar.at(o.kmx); v.kss = (const float *)ar.at(o.kss);
     return v;
 }
 
@@ -773,7 +777,7 @@ int guidedVariant() {
     std::lock_guard<std::mutex> lock(gShapeMu);
     if (gGuidedVariant < 0) {
         const char *e = std::getenv("LGCR_GUIDED_VARIANT");
-        gGuidedVariant = (e && e[0] == '0') ? 0 : 1;
+        gGuidedVariant = (e && e[0] == '1') ? 1 : 0;
     }
     return gGuidedVariant;
 }

@@ -33,6 +33,7 @@ struct AxisView {
     const float *pos, *lpos;
     const int *cbI0, *lbI0;
     const float *cbF, *lbF;
+    const float *kmx, *kss;  // rescue kappa factors per index (separable kernels)
 };
 
 struct RadialView {

@@ -106,15 +106,17 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     const ChromaAxis ax = buildChromaAxis(F.sw, q.outW, rw, q.shiftX, q.k);
     const ChromaAxis ay = buildChromaAxis(F.sh, q.outH, rh, q.shiftY, q.k);
     Image img;
-    struct AxisOff { size_t s, w, wd, am, ws, wa, pos, lpos, ci, cf, li, lf; } oa[2];
+    struct AxisOff { size_t s, w, wd, am, ws, wa, pos, lpos, ci, cf, li, lf, kmx, kss; } oa[2];
     const ChromaAxis *axes[2] = { &ax, &ay };
     for (int i = 0; i < 2; ++i) {
         const ChromaAxis &a = *axes[i];
         const std::vector<double> wd(a.w.begin(), a.w.end());
+        std::vector<float> kmx, kss;
+        rescueFactors(a, kmx, kss);
         oa[i] = { img.add(a.start), img.add(a.w), img.add(wd), img.add(a.am), img.add(a.weightSum),
                   img.add(a.absoluteWeightSum), img.add(a.pos), img.add(a.lpos),
                   img.add(a.chromaBilin.i0), img.add(a.chromaBilin.f),
-                  img.add(a.lumaBilin.i0), img.add(a.lumaBilin.f) };
+                  img.add(a.lumaBilin.i0), img.add(a.lumaBilin.f), img.add(kmx), img.add(kss) };
     }
     RadialTable rad;
     size_t orx = 0, ory = 0, orw = 0;
@@ -176,6 +178,8 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
         v.lpos = (const float *)(base + o.lpos); v.cbI0 = (const int *)(base + o.ci);
         v.cbF = (const float *)(base + o.cf); v.lbI0 = (const int *)(base + o.li);
         v.lbF = (const float *)(base + o.lf);
+        v.kmx = (const float *)(base + o.kmx);
+        v.kss = (const float *)(base + o.kss);
         return v;
     };
     T.ax = axisView(oa[0], ax);
