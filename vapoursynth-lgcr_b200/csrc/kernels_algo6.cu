@@ -232,7 +232,7 @@ k_detail_hpass(LGCR_STAGE_ARGS) {
             continue;
         const float a = ldf(row + iclamp(tx0 + i, 0, J.cw - 1));
         h = fma(__ldg(wx + i), (double)a, h);
-        mn = smin(mn, a); mx = smax(mx, a);
+        mn = runMin(mn, a); mx = runMax(mx, a);
     }
     reinterpret_cast<float4 *>(J.dTab)[(size_t)sy * J.sw + x] = make_float4((float)h, mn, mx, 0.0f);
 }
@@ -261,7 +261,7 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
             const int sy = iclamp(ty0 + j, 0, J.ch - 1);
             const float4 t = __ldg(reinterpret_cast<const float4 *>(J.dTab) + (size_t)sy * J.sw + x);
             v = fma(__ldg(wy + j), (double)t.x, v);
-            mn = smin(mn, t.y); mx = smax(mx, t.z);
+            mn = runMin(mn, t.y); mx = runMax(mx, t.z);
         }
         const double ws = (double)__ldg(ax.wsum + x) * (double)__ldg(ay.wsum + y);
         const double wa = (double)__ldg(ax.wabs + x) * (double)__ldg(ay.wabs + y);
@@ -323,8 +323,8 @@ __device__ __forceinline__ void detailEntry(const float *row, int cw, int tx0, c
             continue;
         const float a = ldf(row + (NOCLAMP ? tx0 + i : iclamp(tx0 + i, 0, cw - 1)));
         acc = fma(w[i], (double)a, acc);
-        lo = smin(lo, a);
-        hi = smax(hi, a);
+        lo = runMin(lo, a);
+        hi = runMax(hi, a);
     }
     hOut = (double)(float)acc;
     ext = make_float2(lo, hi);
@@ -345,8 +345,8 @@ __device__ __forceinline__ double detailVertical(const DetailRows &R, const doub
         const int r = (NOCLAMP ? ty0 + j : iclamp(ty0 + j, 0, ch - 1)) - syLo;
         v = fma(R.w[k][j], sH[r][lx], v);
         const float2 e = sE[r][lx];
-        lo = smin(lo, e.x);
-        hi = smax(hi, e.y);
+        lo = runMin(lo, e.x);
+        hi = runMax(hi, e.y);
     }
     mn = lo;
     mx = hi;

@@ -68,11 +68,11 @@ __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &co
         const double w = col.w[i];
         hU = fma(w, p.x, hU);
         hV = fma(w, p.y, hV);
-        mnU = smin(mnU, p.x); mxU = smax(mxU, p.x);
-        mnV = smin(mnV, p.y); mxV = smax(mxV, p.y);
+        mnU = runMin(mnU, p.x); mxU = runMax(mxU, p.x);
+        mnV = runMin(mnV, p.y); mxV = runMax(mxV, p.y);
         if (lrow) {
             const float l = ldf(lrow + x);
-            mnL = smin(mnL, l); mxL = smax(mxL, l);
+            mnL = runMin(mnL, l); mxL = runMax(mxL, l);
         }
     }
     ea = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
@@ -100,11 +100,11 @@ __device__ __forceinline__ void hEntryGeneric(const FrameJob &J, int ox, int sy,
         const double w = __ldg(wx + i);
         hU = fma(w, p.x, hU);
         hV = fma(w, p.y, hV);
-        mnU = smin(mnU, p.x); mxU = smax(mxU, p.x);
-        mnV = smin(mnV, p.y); mxV = smax(mxV, p.y);
+        mnU = runMin(mnU, p.x); mxU = runMax(mxU, p.x);
+        mnV = runMin(mnV, p.y); mxV = runMax(mxV, p.y);
         if (lrow) {
             const float l = ldf(lrow + x);
-            mnL = smin(mnL, l); mxL = smax(mxL, l);
+            mnL = runMin(mnL, l); mxL = runMax(mxL, l);
         }
     }
     ea = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
@@ -159,8 +159,8 @@ __device__ __forceinline__ void plainFromTableT(const FrameJob &J, int ox, int o
         const double w = __ldg(wy + j);
         vU = fma(w, (double)a.x, vU);
         vV = fma(w, (double)a.y, vV);
-        mnU = smin(mnU, a.z); mxU = smax(mxU, a.w);
-        mnV = smin(mnV, b.x); mxV = smax(mxV, b.y);
+        mnU = runMin(mnU, a.z); mxU = runMax(mxU, a.w);
+        mnV = runMin(mnV, b.x); mxV = runMax(mxV, b.y);
     }
     const double ws = (double)__ldg(ax.wsum + ox) * (double)__ldg(ay.wsum + oy);
     const double wa = (double)__ldg(ax.wabs + ox) * (double)__ldg(ay.wabs + oy);
@@ -242,8 +242,8 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2
         const double w = __ldg(wy + j);
         vU = fma(w, h.x, vU);
         vV = fma(w, h.y, vV);
-        mnU = smin(mnU, e.x); mxU = smax(mxU, e.y);
-        mnV = smin(mnV, e.z); mxV = smax(mxV, e.w);
+        mnU = runMin(mnU, e.x); mxU = runMax(mxU, e.y);
+        mnV = runMin(mnV, e.z); mxV = runMax(mxV, e.w);
     }
     const double ws = (double)__ldg(ax.wsum + ox) * (double)__ldg(ay.wsum + oy);
     const double wa = (double)__ldg(ax.wabs + ox) * (double)__ldg(ay.wabs + oy);
@@ -294,8 +294,8 @@ __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (
         const double w = R.w[k][j];
         vU = fma(w, h.x, vU);
         vV = fma(w, h.y, vV);
-        mnU = smin(mnU, e.x); mxU = smax(mxU, e.y);
-        mnV = smin(mnV, e.z); mxV = smax(mxV, e.w);
+        mnU = runMin(mnU, e.x); mxU = runMax(mxU, e.y);
+        mnV = runMin(mnV, e.z); mxV = runMax(mxV, e.w);
     }
     const double ws = (double)wsX * (double)R.wsum[k];
     const double wa = (double)waX * (double)R.wabs[k];
@@ -548,38 +548,6 @@ __device__ __forceinline__ void tap(const TapCtx &c, size_t o, float dxf, float 
     tapCore<true>(c, ldf(c.lc + o), __ldg(c.uv + o), dx * c.nx, -dx * c.ny, dy_ny, dy_nx, wx, a);
 }
 
-// Two taps' FP32 arithmetic per instruction: the packed f32x2 add, sub, mul
-// and fma of sm_100 round each lane exactly like the scalar instruction.
-typedef unsigned long long f32x2;
-
-__device__ __forceinline__ f32x2 pk2(float a, float b) {
-    f32x2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ void up2(f32x2 r, float &a, float &b) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-}
-__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
-    f32x2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
 // rcpInRange on both lanes: hardware approximation per lane, then the same
 // fused Newton-Raphson refinement e = 1 - x*y, y' = y + y*e on the pair.
 __device__ __forceinline__ f32x2 rcp2(f32x2 x, f32x2 one) {
@@ -704,9 +672,9 @@ __device__ __forceinline__ void windowExtrema(const FrameJob &J, int ox, int ty0
         const int sy = J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1);
         const float4 *h = reinterpret_cast<const float4 *>(J.hTab + ((size_t)sy * J.W + ox) * 8);
         const float4 a = __ldg(h), b = __ldg(h + 1);
-        mnU = smin(mnU, a.z); mxU = smax(mxU, a.w);
-        mnV = smin(mnV, b.x); mxV = smax(mxV, b.y);
-        mnL = smin(mnL, b.z); mxL = smax(mxL, b.w);
+        mnU = runMin(mnU, a.z); mxU = runMax(mxU, a.w);
+        mnV = runMin(mnV, b.x); mxV = runMax(mxV, b.y);
+        mnL = runMin(mnL, b.z); mxL = runMax(mxL, b.w);
     }
     ext[0] = mnU; ext[1] = mxU; ext[2] = mnV; ext[3] = mxV; ext[4] = mnL; ext[5] = mxL;
 }

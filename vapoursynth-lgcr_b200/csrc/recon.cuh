@@ -161,6 +161,19 @@ template <class T> __device__ __forceinline__ T sclamp(T v, T lo, T hi) {
 }
 __device__ __forceinline__ int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Running minimum / maximum of an accumulator that starts at +-1e30 (never
+// NaN). Float: the hardware min/max (one instruction) returns what the
+// reference's std::min/std::max return -- a NaN sample leaves the
+// accumulator unchanged either way -- except possibly the sign of a zero
+// result, which no output can show (every use is a clamp bound or |x - L0|,
+// and the output stores normalise -0 as the reference's s * 1.0 + 0.0 does).
+// Double: the std::min/std::max select itself (cheaper here than the
+// library fmin/fmax).
+__device__ __forceinline__ float runMin(float acc, float v) { return fminf(acc, v); }
+__device__ __forceinline__ float runMax(float acc, float v) { return fmaxf(acc, v); }
+__device__ __forceinline__ double runMin(double acc, double v) { return (v < acc) ? v : acc; }
+__device__ __forceinline__ double runMax(double acc, double v) { return (acc < v) ? v : acc; }
+
 __device__ __forceinline__ float ldf(const float *p) { return __ldg(p); }
 
 // 1/x for denominators of the form 1 + (non-negative terms), i.e. x >= 1,
@@ -191,6 +204,38 @@ __device__ __forceinline__ float rcpAtLeastOne(float x) {
     return rcpOutOfRange(x);
 }
 
+// Two lanes of FP32 arithmetic per instruction: the packed f32x2 add, sub,
+// mul and fma of sm_100 round each lane exactly like the scalar instruction.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void up2(f32x2 r, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
 // Dilated trust mask bit of luma sample (x, y).
 __device__ __forceinline__ uint32_t maskAt(const FrameJob &J, int x, int y) {
     return (__ldg(J.mask + (size_t)y * J.maskWords + (x >> 5)) >> (x & 31)) & 1u;
