@@ -73,6 +73,7 @@ struct DeviceTables {
     int bmAnchorsX = 0, bmAnchorsY = 0;
     int axSup = 0, aySup = 0;
     int plainMaxRows = 0;               // most chroma rows one k_plain block reads
+    int plainRows = 0;                  // output rows per k_plain block
     int detailMaxRows = 0;              // most chroma rows one k_detail_map block reads
     int sAxSup = 0, sAySup = 0;         // source-grid axis supports (algo 6)
     int ycMaxRows = 0, ycMaxSup = 0;    // candidate tables: rows per k_yc_tiled block, widest support

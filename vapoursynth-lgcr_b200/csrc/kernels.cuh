@@ -11,7 +11,8 @@ namespace lgcr_b200 {
 
 // k_plain: output rows per block (32 columns wide, 32x8 threads) and the
 // most horizontal-table rows one block stages in shared memory.
-constexpr int kPlainRows = 32;
+constexpr int kPlainRows = 64;          // tall blocks (frames whose windows fit)
+constexpr int kPlainRowsShort = 32;     // other frames
 constexpr int kPlainStagedRows = 40;
 
 // k_convert: samples per warp (one row segment) and warps per block; the

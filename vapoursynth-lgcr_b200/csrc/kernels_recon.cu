@@ -264,7 +264,7 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2
 }
 
 // Per-row vertical tap data of one k_plain block, staged once for the
-// block's kPlainRows output rows (supports up to 8 taps).
+// block's output rows (at most kPlainRows; supports up to 8 taps).
 struct PlainRows {
     double w[kPlainRows][8];
     int ty0[kPlainRows];
@@ -370,7 +370,7 @@ __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int 
 }
 
 // Plain stage: every pixel the guided pass does not finalize. A block covers
-// 32 output columns x kPlainRows output rows. For the separable kernels it
+// 32 output columns x J.plainRows output rows. For the separable kernels it
 // needs the horizontal entries of the chroma rows its windows touch:
 //  * fused frames (every block's rows fit in shared memory) compute them
 //    here from the chroma planes (the reference's ring rows), and write the
@@ -393,8 +393,8 @@ k_plain(LGCR_STAGE_ARGS) {
     const int tile = blockIdx.x - tileStart[f];
     const int tilesX = (J.W + 31) >> 5;
     const int colBase = (tile % tilesX) * 32;
-    const int oy0 = (tile / tilesX) * kPlainRows;
-    const int rowsHere = min(kPlainRows, J.H - oy0);
+    const int oy0 = (tile / tilesX) * J.plainRows;
+    const int rowsHere = min(J.plainRows, J.H - oy0);
     const int lx = threadIdx.x;
     const int ox = colBase + lx;
     const int tid = threadIdx.y * 32 + lx;
@@ -434,8 +434,8 @@ k_plain(LGCR_STAGE_ARGS) {
         R.maskWord[tid] = __ldg(J.mask + (size_t)(oy0 + tid) * J.maskWords + (colBase >> 5));
     if (fused) {
         // rows from the next block's first row on belong to the next block
-        const int syOwnEnd = (oy0 + kPlainRows < J.H)
-            ? iclamp(__ldg(J.ay.start + oy0 + kPlainRows), 0, J.ch - 1) : J.ch;
+        const int syOwnEnd = (oy0 + J.plainRows < J.H)
+            ? iclamp(__ldg(J.ay.start + oy0 + J.plainRows), 0, J.ch - 1) : J.ch;
         const bool writeTable = J.listed && J.hTab;
         if (ox < J.W) {
             switch (J.ax.sup) {

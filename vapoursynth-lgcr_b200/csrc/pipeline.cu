@@ -389,11 +389,22 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
     t->ay = axisView(t->arena, oay);
     t->axSup = ax.sup;
     t->aySup = ay.sup;
-    for (int oy0 = 0; oy0 < p.outH; oy0 += kPlainRows) {
-        const int oyLast = std::min(oy0 + kPlainRows, p.outH) - 1;
-        const int lo = std::clamp(ay.start[oy0], 0, ch - 1);
-        const int hi = std::clamp(ay.start[oyLast] + ay.sup - 1, 0, ch - 1);
-        t->plainMaxRows = std::max(t->plainMaxRows, hi - lo + 1);
+    // k_plain blocks: tall when every block's chroma rows fit in shared memory
+    auto plainRowsRead = [&](int rows) {
+        int most = 0;
+        for (int oy0 = 0; oy0 < p.outH; oy0 += rows) {
+            const int oyLast = std::min(oy0 + rows, p.outH) - 1;
+            const int lo = std::clamp(ay.start[oy0], 0, ch - 1);
+            const int hi = std::clamp(ay.start[oyLast] + ay.sup - 1, 0, ch - 1);
+            most = std::max(most, hi - lo + 1);
+        }
+        return most;
+    };
+    t->plainRows = kPlainRows;
+    t->plainMaxRows = plainRowsRead(kPlainRows);
+    if (t->plainMaxRows > kPlainStagedRows) {
+        t->plainRows = kPlainRowsShort;
+        t->plainMaxRows = plainRowsRead(kPlainRowsShort);
     }
     if (p.k.radial)
         t->rad = radialView(t->arena, orad);
@@ -661,6 +672,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         J.bumpRcpSafe = bound < 1.0e18 ? 1 : 0;
     }
     J.plainFused = (J.hTab && !J.radial && T.plainMaxRows <= kPlainStagedRows) ? 1 : 0;
+    J.plainRows = J.plainFused ? T.plainRows : kPlainRowsShort;
     {
         // every tap index in range: starts lie in [0, srcChromaN - sup] and the
         // integer-ratio chroma count equals the plane size
@@ -824,7 +836,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_HPASS: return (J.hTab && !J.radial && !J.plainFused && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
-    case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, kPlainRows);
+    case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, J.plainRows);
     case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC: return (J.guided && J.algo == 6 && !J.ycTiled) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_YC_TILED: return (J.guided && J.algo == 6 && J.ycTiled) ? cdiv(J.cw, kYcTile) * cdiv(J.ch, kYcTile) : 0;

@@ -115,6 +115,7 @@ struct __align__(16) FrameJob {
     int listed;                        // frame uses the guided work list
     int bumpRcpSafe;                   // every guided bump denominator stays below 2^64
     int plainFused;                    // k_plain computes its horizontal rows itself
+    int plainRows;                     // output rows per k_plain block
     int noClampX, noClampY;            // every chroma tap index is in range
     // algo 6 / algo 4 / bm workspaces
     float *aff;                        // 9 chroma planes: aU aV g mnU mxU mnV mxV rng dgl
