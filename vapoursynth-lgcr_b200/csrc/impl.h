@@ -75,6 +75,7 @@ struct DeviceTables {
     int plainMaxRows = 0;               // most chroma rows one k_plain block reads
     int plainRows = 0;                  // output rows per k_plain block
     int detailMaxRows = 0;              // most chroma rows one k_detail_map block reads
+    int detailRows = 0;                 // output rows per k_detail_map block
     int sAxSup = 0, sAySup = 0;         // source-grid axis supports (algo 6)
     int ycMaxRows = 0, ycMaxSup = 0;    // candidate tables: rows per k_yc_tiled block, widest support
 };

@@ -64,8 +64,10 @@ __global__ void k_affine(LGCR_STAGE_ARGS);
 __global__ void k_detail_hpass(LGCR_STAGE_ARGS);
 __global__ void k_detail_plain(LGCR_STAGE_ARGS);
 __global__ void k_detail_nyq(LGCR_STAGE_ARGS, int pass);
-// k_detail_map: output samples per block side (32 computed with the halo).
+// k_detail_map: output columns per block (32 computed with the halo) and
+// output rows per block: tall when the tile's chroma rows fit, else short.
 constexpr int kDetailTile = 30;
+constexpr int kDetailRowsTall = 62;
 __global__ void k_detail_map(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_h(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_v(LGCR_STAGE_ARGS);

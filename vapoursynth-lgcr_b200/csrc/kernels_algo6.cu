@@ -292,17 +292,18 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
 // Fused detail map (separable kernels, supports up to 8 taps): the horizontal
 // pass of the degraded luma into shared memory, the vertical pass and
 // detail = Y - plain(D(Y)), then the Nyquist passes (at most one per axis:
-// chroma ratios are at most 2) on a 32 x 32 tile with a one-sample halo; the
-// block writes the 30 x 30 interior to the detail plane. Tile samples sit at
+// chroma ratios are at most 2) on a 32-wide tile with a one-sample halo; the
+// block writes the 30-column interior of J.detailRows rows (62, or 30 when
+// the taller tile's chroma rows do not fit) to the detail plane. Samples sit at
 // clamped coordinates, so at the plane borders the halo holds exactly the
 // clamped neighbours the reference's passes read (buildDetailMap,
 // src/algos.cpp:1528-1585, with suppressSourceNyquist 1303-1364).
 // ---------------------------------------------------------------------------
 struct DetailRows {
-    double w[32][8];
-    int ty0[32], r[32];
-    uint32_t act[32];
-    float wsum[32], wabs[32], pos[32];
+    double w[kDetailRowsTall + 2][8];
+    int ty0[kDetailRowsTall + 2], r[kDetailRowsTall + 2];
+    uint32_t act[kDetailRowsTall + 2];
+    float wsum[kDetailRowsTall + 2], wabs[kDetailRowsTall + 2], pos[kDetailRowsTall + 2];
 };
 
 __device__ __forceinline__ uint32_t activityBits(const uint8_t *am, int n) {
@@ -357,8 +358,8 @@ __global__ void __launch_bounds__(256)
 k_detail_map(LGCR_STAGE_ARGS) {
     __shared__ double sH[kPlainStagedRows][32];
     __shared__ float2 sE[kPlainStagedRows][32];
-    __shared__ float sD[32][33];
-    __shared__ float sX[32][33];
+    __shared__ float sD[kDetailRowsTall + 2][33];
+    __shared__ float sX[kDetailRowsTall + 2][33];
     __shared__ DetailRows R;
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -366,18 +367,19 @@ k_detail_map(LGCR_STAGE_ARGS) {
     const FrameJob &J = sJob;
     const int tile = blockIdx.x - tileStart[f];
     const int w = J.sw, h = J.sh, cw = J.cw, ch = J.ch;
+    const int rowsOut = J.detailRows, rowsIn = rowsOut + 2;
     const int tilesX = (w + kDetailTile - 1) / kDetailTile;
-    const int x0 = (tile % tilesX) * kDetailTile, y0 = (tile / tilesX) * kDetailTile;
+    const int x0 = (tile % tilesX) * kDetailTile, y0 = (tile / tilesX) * rowsOut;
     const int lx = threadIdx.x, tid = threadIdx.y * 32 + lx;
     const int c = iclamp(x0 - 1 + lx, 0, w - 1);
     const AxisView &ax = J.sax, &ay = J.say;
     const int supY = ay.sup;
-    for (int i = tid; i < 32 * supY; i += 256) {
+    for (int i = tid; i < rowsIn * supY; i += 256) {
         const int k = i / supY, j = i - k * supY;
         const int rk = iclamp(y0 - 1 + k, 0, h - 1);
         R.w[k][j] = __ldg(ay.wd + (size_t)rk * supY + j);
     }
-    if (tid < 32) {
+    if (tid < rowsIn) {
         const int rk = iclamp(y0 - 1 + tid, 0, h - 1);
         R.r[tid] = rk;
         R.ty0[tid] = __ldg(ay.start + rk);
@@ -387,7 +389,7 @@ k_detail_map(LGCR_STAGE_ARGS) {
         R.pos[tid] = __ldg(ay.pos + rk);
     }
     const int syLo = iclamp(__ldg(ay.start + iclamp(y0 - 1, 0, h - 1)), 0, ch - 1);
-    const int syHi = iclamp(__ldg(ay.start + iclamp(y0 + kDetailTile, 0, h - 1)) + supY - 1, 0, ch - 1);
+    const int syHi = iclamp(__ldg(ay.start + iclamp(y0 + rowsOut, 0, h - 1)) + supY - 1, 0, ch - 1);
     const int nRows = syHi - syLo + 1;
     const float *dgl = J.aff + 8 * (size_t)cw * ch;
     {
@@ -414,7 +416,7 @@ k_detail_map(LGCR_STAGE_ARGS) {
     __syncthreads();
     {
         const float wsX = __ldg(ax.wsum + c), waX = __ldg(ax.wabs + c), posX = __ldg(ax.pos + c);
-        for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        for (int k = threadIdx.y; k < rowsIn; k += blockDim.y) {
             float mn, mx;
             double v = J.sNoClampY ? detailVertical<true>(R, sH, sE, k, lx, syLo, ch, mn, mx)
                                    : detailVertical<false>(R, sH, sE, k, lx, syLo, ch, mn, mx);
@@ -433,7 +435,7 @@ k_detail_map(LGCR_STAGE_ARGS) {
     const float (*src)[33] = sD;
     if (J.nyqX) {
         if (lx >= 1 && lx <= kDetailTile)
-            for (int k = threadIdx.y; k < 32; k += blockDim.y)
+            for (int k = threadIdx.y; k < rowsIn; k += blockDim.y)
                 sX[k][lx] = 0.25f * sD[k][lx - 1] + 0.5f * sD[k][lx] + 0.25f * sD[k][lx + 1];
         __syncthreads();
         src = sX;
@@ -442,7 +444,7 @@ k_detail_map(LGCR_STAGE_ARGS) {
     if (lx < 1 || lx > kDetailTile || x >= w)
         return;
     float *dst = const_cast<float *>(J.detailSrc);
-    for (int k = 1 + threadIdx.y; k <= kDetailTile; k += blockDim.y) {
+    for (int k = 1 + threadIdx.y; k <= rowsOut; k += blockDim.y) {
         const int y = y0 - 1 + k;
         if (y >= h)
             break;

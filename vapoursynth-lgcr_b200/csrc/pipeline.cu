@@ -337,11 +337,21 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         osay = packAxis(pk, say);
         t->sAxSup = sax.sup;
         t->sAySup = say.sup;
-        for (int y0 = 0; y0 < sh; y0 += kDetailTile) {
-            const int r0 = std::clamp(y0 - 1, 0, sh - 1), r1 = std::clamp(y0 + kDetailTile, 0, sh - 1);
-            const int lo = std::clamp(say.start[r0], 0, ch - 1);
-            const int hi = std::clamp(say.start[r1] + say.sup - 1, 0, ch - 1);
-            t->detailMaxRows = std::max(t->detailMaxRows, hi - lo + 1);
+        auto detailRowsRead = [&](int rows) {
+            int most = 0;
+            for (int y0 = 0; y0 < sh; y0 += rows) {
+                const int r0 = std::clamp(y0 - 1, 0, sh - 1), r1 = std::clamp(y0 + rows, 0, sh - 1);
+                const int lo = std::clamp(say.start[r0], 0, ch - 1);
+                const int hi = std::clamp(say.start[r1] + say.sup - 1, 0, ch - 1);
+                most = std::max(most, hi - lo + 1);
+            }
+            return most;
+        };
+        t->detailRows = kDetailRowsTall;
+        t->detailMaxRows = detailRowsRead(kDetailRowsTall);
+        if (t->detailMaxRows > kPlainStagedRows) {
+            t->detailRows = kDetailTile;
+            t->detailMaxRows = detailRowsRead(kDetailTile);
         }
         if (p.k.radial)
             osrad = packRadial(pk, buildRadialTable(p.k, sax, say, cw, ch));
@@ -699,6 +709,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         J.sNoClampX = (nx == F.cw && F.cw >= T.sAxSup) ? 1 : 0;
         J.sNoClampY = (ny == F.ch && F.ch >= T.sAySup) ? 1 : 0;
         J.ycTiled = (T.ycMaxSup <= 8 && T.ycMaxRows <= kYcRows) ? 1 : 0;
+        J.detailRows = T.detailRows;
         J.detailFused = (J.dTab && !J.radial && J.kernel != 0 && T.sAxSup <= 8 && T.sAySup <= 8 &&
                          T.detailMaxRows <= kPlainStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
     }
@@ -843,7 +854,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_PLAIN: return (J.guided && J.algo == 6 && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
-    case S_DET_MAP: return (J.guided && J.algo == 6 && J.detailFused) ? cdiv(J.sw, kDetailTile) * cdiv(J.sh, kDetailTile) : 0;
+    case S_DET_MAP: return (J.guided && J.algo == 6 && J.detailFused) ? cdiv(J.sw, kDetailTile) * cdiv(J.sh, J.detailRows) : 0;
     case S_DET_RH: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_RV: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_DET_RR: return (J.guided && J.algo == 6 && resize && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
