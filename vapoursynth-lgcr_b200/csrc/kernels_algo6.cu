@@ -193,19 +193,16 @@ k_affine(LGCR_STAGE_ARGS) {
         q[k] = sclamp((covU * covU + covV * covV) / ((varY + eps) * (varU + varV + eps)), 0.0, 1.0);
     }
     const size_t C = (size_t)w * h;
-    float *A = J.aff;
-    A[0 * C + o] = median3f((float)aU[0], (float)aU[1], (float)aU[2]);
-    A[1 * C + o] = median3f((float)aV[0], (float)aV[1], (float)aV[2]);
+    const float slopeU = median3f((float)aU[0], (float)aU[1], (float)aU[2]);
+    const float slopeV = median3f((float)aV[0], (float)aV[1], (float)aV[2]);
     const double qmax = smax(smax(q[0], q[1]), q[2]);
     const double qmin = smin(smin(q[0], q[1]), q[2]);
     const double stability = qmax > 1e-9 ? qmin / qmax : 0.0;
     const double chromaSignal = (varU + varV) / (varU + varV + epsSig);
-    A[2 * C + o] = (float)(((q[0] + q[1] + q[2]) / 3.0) * stability * chromaSignal);
-    A[3 * C + o] = mnU;
-    A[4 * C + o] = mxU;
-    A[5 * C + o] = mnV;
-    A[6 * C + o] = mxV;
-    A[7 * C + o] = smax(mxU - mnU, mxV - mnV);
+    const float gain = (float)(((q[0] + q[1] + q[2]) / 3.0) * stability * chromaSignal);
+    // interleaved maps: (aU, aV, g, rng) then (mnU, mxU, mnV, mxV) per sample
+    reinterpret_cast<float4 *>(J.aff)[o] = make_float4(slopeU, slopeV, gain, smax(mxU - mnU, mxV - mnV));
+    reinterpret_cast<float4 *>(J.aff + 4 * C)[o] = make_float4(mnU, mxU, mnV, mxV);
 }
 
 // Horizontal pass of the degraded-luma reconstruction (separable kernels):
@@ -572,14 +569,16 @@ __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
     const float cxf = __ldg(ax.cbF + ox), cyf = __ldg(ay.cbF + oy);
     const int cw = J.cw, ch = J.ch;
     const size_t C = (size_t)cw * ch;
-    const float q = bilinearFast(J.aff + 2 * C, cw, ch, cxi, cxf, cyi, cyf);
+    // (aU, aV, g, rng) and (mnU, mxU, mnV, mxV), bilinear per component
+    const float4 amap = bilinearFast4(reinterpret_cast<const float4 *>(J.aff), cw, ch, cxi, cxf, cyi, cyf);
+    const float q = amap.z;
     float g = (1.0f - J.qgate * (1.0f - q)) * J.strength;
     if (J.useMs) {
         const float ms = bilinearFast(J.ms, cw, ch, cxi, cxf, cyi, cyf);
         g *= 1.0f - J.msStrength * (1.0f - ms);
     }
-    const float au = bilinearFast(J.aff + 0 * C, cw, ch, cxi, cxf, cyi, cyf);
-    const float av = bilinearFast(J.aff + 1 * C, cw, ch, cxi, cxf, cyi, cyf);
+    const float au = amap.x;
+    const float av = amap.y;
     const float coherence = dir.coherence;
     const float tx = -dir.ny, ty = dir.nx;
     const float *dl = J.detail;
@@ -589,7 +588,7 @@ __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
     const float dtm = bilinearAt(dl, J.W, J.H, (float)ox - tx * s, (float)oy - ty * s);
     const float dt = 0.25f * dtp + 0.5f * dc + 0.25f * dtm;
     const float det = dc + (dt - dc) * coherence;
-    const float cap = 0.5f * bilinearFast(J.aff + 7 * C, cw, ch, cxi, cxf, cyi, cyf);
+    const float cap = 0.5f * amap.w;
     const float cu = sclamp(g * au * det, -cap, cap);
     const float cv = sclamp(g * av * det, -cap, cap);
     const size_t o = (size_t)oy * J.W + ox;
@@ -597,10 +596,12 @@ __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
     float ou = ru + cu, ov = rv + cv;
     if (J.clampHull) {
         const float ar = J.margin;
-        const float loU = smin(ru, bilinearFast(J.aff + 3 * C, cw, ch, cxi, cxf, cyi, cyf) - ar);
-        const float hiU = smax(ru, bilinearFast(J.aff + 4 * C, cw, ch, cxi, cxf, cyi, cyf) + ar);
-        const float loV = smin(rv, bilinearFast(J.aff + 5 * C, cw, ch, cxi, cxf, cyi, cyf) - ar);
-        const float hiV = smax(rv, bilinearFast(J.aff + 6 * C, cw, ch, cxi, cxf, cyi, cyf) + ar);
+        const float4 hull = bilinearFast4(reinterpret_cast<const float4 *>(J.aff + 4 * C), cw, ch, cxi,
+                                          cxf, cyi, cyf);
+        const float loU = smin(ru, hull.x - ar);
+        const float hiU = smax(ru, hull.y + ar);
+        const float loV = smin(rv, hull.z - ar);
+        const float hiV = smax(rv, hull.w + ar);
         ou = sclamp(ou, loU, hiU);
         ov = sclamp(ov, loV, hiV);
     }

@@ -118,7 +118,8 @@ struct __align__(16) FrameJob {
     int plainRows;                     // output rows per k_plain block
     int noClampX, noClampY;            // every chroma tap index is in range
     // algo 6 / algo 4 / bm workspaces
-    float *aff;                        // 9 chroma planes: aU aV g mnU mxU mnV mxV rng dgl
+    float *aff;                        // cw x ch: float4 (aU aV g rng), float4 (mnU mxU
+                                       // mnV mxV) per sample, then the dgl plane at 8*C
     float *yc1, *yc2;                  // bilinear / bicubic degradation candidates
     float *ycTmp;                      // cw x sh candidate intermediate (resize case)
     float *detail;                     // sw x sh (or W x H) detail map
@@ -297,6 +298,35 @@ __device__ __forceinline__ float bilinearFast(const float *p, int w, int h, int 
     const float *r1 = r0 + w;
     const float a = ldf(r0), b = ldf(r0 + 1), c = ldf(r1), d = ldf(r1 + 1);
     return a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+}
+
+// bilinearFast of four interleaved planes (float4 per sample): the same
+// loads' positions and the same arithmetic per component.
+__device__ __forceinline__ float4 bl4(float4 a, float4 b, float4 c, float4 d, float fx, float fy) {
+    return make_float4(a.x + (b.x - a.x) * fx + (c.x - a.x) * fy + (a.x - b.x - c.x + d.x) * fx * fy,
+                       a.y + (b.y - a.y) * fx + (c.y - a.y) * fy + (a.y - b.y - c.y + d.y) * fx * fy,
+                       a.z + (b.z - a.z) * fx + (c.z - a.z) * fy + (a.z - b.z - c.z + d.z) * fx * fy,
+                       a.w + (b.w - a.w) * fx + (c.w - a.w) * fy + (a.w - b.w - c.w + d.w) * fx * fy);
+}
+
+__device__ __forceinline__ float4 bilinearFast4(const float4 *p, int w, int h, int x0, float fx,
+                                                int y0, float fy) {
+    if (w == 1) {
+        const float4 a = __ldg(p + (size_t)y0 * w);
+        if (h == 1)
+            return a;
+        const float4 c = __ldg(p + (size_t)(y0 + 1) * w);
+        return make_float4(a.x + (c.x - a.x) * fy, a.y + (c.y - a.y) * fy, a.z + (c.z - a.z) * fy,
+                           a.w + (c.w - a.w) * fy);
+    }
+    const float4 *r0 = p + (size_t)y0 * w + x0;
+    if (h == 1) {
+        const float4 a = __ldg(r0), b = __ldg(r0 + 1);
+        return make_float4(a.x + (b.x - a.x) * fx, a.y + (b.y - a.y) * fx, a.z + (b.z - a.z) * fx,
+                           a.w + (b.w - a.w) * fx);
+    }
+    const float4 *r1 = r0 + w;
+    return bl4(__ldg(r0), __ldg(r0 + 1), __ldg(r1), __ldg(r1 + 1), fx, fy);
 }
 
 struct TensorDir { float coherence, nx, ny; };
