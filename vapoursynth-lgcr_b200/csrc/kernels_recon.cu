@@ -54,10 +54,13 @@ template <int SUP, bool NOCLAMP>
 __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &col, int sy, float4 &ea,
                                        float4 &eb) {
     const int cw = J.cw;
-    const double2 *uv = reinterpret_cast<const double2 *>(J.uvd) + (size_t)sy * cw;
-    const float *lrow = J.lc ? J.lc + (size_t)sy * cw : nullptr;
+    const size_t row = (size_t)sy * cw;
+    const double2 *uv = reinterpret_cast<const double2 *>(J.uvd) + row;
+    const float *urow = J.U + row, *vrow = J.V + row;
+    const float *lrow = J.lc ? J.lc + row : nullptr;
     double hU = 0.0, hV = 0.0;
-    double mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+    // extrema of the float samples (the doubles hold the same values)
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
     float mnL = 1e30f, mxL = -1e30f;
 #pragma unroll
     for (int i = 0; i < SUP; ++i) {
@@ -68,15 +71,16 @@ __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &co
         const double w = col.w[i];
         hU = fma(w, p.x, hU);
         hV = fma(w, p.y, hV);
-        mnU = runMin(mnU, p.x); mxU = runMax(mxU, p.x);
-        mnV = runMin(mnV, p.y); mxV = runMax(mxV, p.y);
+        const float u = ldf(urow + x), v = ldf(vrow + x);
+        mnU = runMin(mnU, u); mxU = runMax(mxU, u);
+        mnV = runMin(mnV, v); mxV = runMax(mxV, v);
         if (lrow) {
             const float l = ldf(lrow + x);
             mnL = runMin(mnL, l); mxL = runMax(mxL, l);
         }
     }
-    ea = make_float4((float)hU, (float)hV, (float)mnU, (float)mxU);
-    eb = make_float4((float)mnV, (float)mxV, mnL, mxL);
+    ea = make_float4((float)hU, (float)hV, mnU, mxU);
+    eb = make_float4(mnV, mxV, mnL, mxL);
 }
 
 // Any support (activity read per tap).
