@@ -635,8 +635,16 @@ k_lgf(LGCR_STAGE_ARGS) {
     if (x >= w || y >= h)
         return;
     const size_t o = (size_t)y * w + x;
-    if (J.lgfRoiOnly && J.roi[o] == 0)
+    if (J.lgfRoiOnly && J.roi[o] == 0) {
+        // outside the ROI the maps hold zeros (buildLGFMaps fills them before
+        // the ROI pass, recon.cpp:1541-1548); the blend reads them wherever
+        // w2 or w3 reaches 1e-4, which includes samples outside the ROI
+        const size_t C = (size_t)w * h;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            J.lgf[k * C + o] = 0.0f;
         return;
+    }
     const int top = max(0, y - 2), bottom = min(h - 1, y + 2);
     const int left = max(0, x - 2), right = min(w - 1, x + 2);
     double s[6] = {0, 0, 0, 0, 0, 0};

@@ -45,6 +45,57 @@ __device__ __forceinline__ float rawToFloat(uint32_t raw, double scale, double o
     return KIND == kF32 ? __uint_as_float(raw) : (float)((double)raw * scale + off);
 }
 
+// Eight consecutive raw samples from one 16-byte (u16, f32: two) or 8-byte
+// (u8) aligned load; false when the address is not aligned.
+template <int KIND>
+__device__ __forceinline__ bool rawLoad8(const char *row, int x, uint32_t (&raw)[8]) {
+    constexpr int bps = KIND == kF32 ? 4 : (KIND == kU16 ? 2 : 1);
+    const char *p = row + (size_t)x * bps;
+    if (KIND == kU8) {
+        if (reinterpret_cast<uintptr_t>(p) & 7)
+            return false;
+        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(p));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            raw[k] = (q.x >> (8 * k)) & 0xffu;
+            raw[4 + k] = (q.y >> (8 * k)) & 0xffu;
+        }
+        return true;
+    }
+    if (reinterpret_cast<uintptr_t>(p) & 15)
+        return false;
+    if (KIND == kU16) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p));
+        const uint32_t w[4] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            raw[2 * k] = w[k] & 0xffffu;
+            raw[2 * k + 1] = w[k] >> 16;
+        }
+        return true;
+    }
+    const uint4 a = __ldg(reinterpret_cast<const uint4 *>(p)), b = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+    raw[0] = a.x; raw[1] = a.y; raw[2] = a.z; raw[3] = a.w;
+    raw[4] = b.x; raw[5] = b.y; raw[6] = b.z; raw[7] = b.w;
+    return true;
+}
+
+template <int KIND>
+__device__ __forceinline__ void rawStore8(char *row, int x, const uint32_t (&raw)[8]) {
+    constexpr int bps = KIND == kF32 ? 4 : (KIND == kU16 ? 2 : 1);
+    char *p = row + (size_t)x * bps;
+    if (KIND == kU16 && !(reinterpret_cast<uintptr_t>(p) & 15)) {
+        *reinterpret_cast<uint4 *>(p) = make_uint4(raw[0] | raw[1] << 16, raw[2] | raw[3] << 16,
+                                                   raw[4] | raw[5] << 16, raw[6] | raw[7] << 16);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        rawStore<KIND>(row, x + k, raw[k]);
+}
+
+// Luma: each lane converts 8 consecutive samples (one vector load) of the
+// warp's 256-sample row segment; unaligned rows take the per-sample path.
 template <int KIND>
 __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, int lane) {
     const char *src = static_cast<const char *>(J.in[0]) + (long long)y * J.inPitch[0];
@@ -53,16 +104,35 @@ __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, in
     float *yw = J.Yw ? J.Yw + (size_t)y * J.sw : nullptr;
     const double scale = J.yScale;
     const int w = J.sw;
-#pragma unroll 4
-    for (int k = 0; k < kConvertSpan / 32; ++k) {
-        const int x = xb + lane + 32 * k;
-        if (x >= w)
-            break;
-        const uint32_t raw = rawLoad<KIND>(src, x);
-        if (yw)
-            yw[x] = rawToFloat<KIND>(raw, scale, 0.0);
+    const int x = xb + lane * 8;
+    if (x >= w)
+        return;
+    uint32_t raw[8];
+    if (x + 8 <= w && rawLoad8<KIND>(src, x, raw)) {
+        if (yw) {
+            float v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                v[k] = rawToFloat<KIND>(raw[k], scale, 0.0);
+            if (!(reinterpret_cast<uintptr_t>(yw + x) & 15)) {
+                reinterpret_cast<float4 *>(yw + x)[0] = make_float4(v[0], v[1], v[2], v[3]);
+                reinterpret_cast<float4 *>(yw + x)[1] = make_float4(v[4], v[5], v[6], v[7]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    yw[x + k] = v[k];
+            }
+        }
         if (dst)
-            rawStore<KIND>(dst, x, raw);
+            rawStore8<KIND>(dst, x, raw);
+        return;
+    }
+    for (int k = 0; k < 8 && x + k < w; ++k) {
+        const uint32_t r = rawLoad<KIND>(src, x + k);
+        if (yw)
+            yw[x + k] = rawToFloat<KIND>(r, scale, 0.0);
+        if (dst)
+            rawStore<KIND>(dst, x + k, r);
     }
 }
 

@@ -506,6 +506,12 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     }
     if (!ar.commit())
         return nullptr;
+    // LGCR_POISON_WORKSPACE=1: fill new workspaces with 0xFF bytes (NaN
+    // floats, -1 integers), so a stage that reads scratch no stage wrote
+    // shows in the output instead of depending on earlier frames
+    if (const char *e = std::getenv("LGCR_POISON_WORKSPACE"); e && e[0] == '1')
+        if (cudaMemset(ar.at(0), 0xFF, ar.size()) != cudaSuccess)
+            return nullptr;
     auto F = [&](const Slot &s) { return s.on ? (float *)ar.at(s.off) : nullptr; };
     auto B = [&](const Slot &s) { return s.on ? (uint8_t *)ar.at(s.off) : nullptr; };
     ws->dJob = (FrameJob *)ar.at(sJob.off);
