@@ -16,6 +16,10 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
   roofline     dominant stage: algorithmic bytes (9 B per output pixel for
                10-bit 4:2:0 -> 4:4:4) / its CUDA-event duration vs measured HBM
   cpu_baseline the reference's AVX2 build on this host's cores (bounded sample)
+  serving      the serving configuration's mixed stream (5 frame kinds, algo
+               2/4/6, bm on 10 %, 24 streams) as Poisson arrivals at 1.2x the
+               per-frame path's capacity into the continuous-batching server
+               (8 GB budget): throughput and p50/p99/p99.9 latency
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -238,6 +242,131 @@ def reference_arm(args):
     }
     print(json.dumps(line))
     return 0
+
+
+# ---------------------------------------------------------------------------
+# serving leg: the mixed request stream of the serving configuration
+# ---------------------------------------------------------------------------
+SERVE_KINDS = [
+    ("1280x720 YUV420P8", 1280, 720, S.YUV420P8, {}, {}),
+    ("1920x1080 YUV422P10", 1920, 1080, S.YUV422P10, {}, {}),
+    ("3840x2160 YUV420P10", 3840, 2160, S.YUV420P10, {}, {}),
+    ("1920x1080 YUV444PS", 1920, 1080, S.YUV444PS, {"blur_chroma": True}, {}),
+    ("1920x1080->3840x2160 YUV420P10 jinc", 1920, 1080, S.YUV420P10, {},
+     {"kernel": "jinc", "taps": 3, "width": 3840, "height": 2160}),
+]
+SERVE_STREAMS = 24
+SERVE_SEEDS = 4          # content seeds per frame kind shared by the streams
+SERVE_RING = 16          # host output buffers per kind
+
+
+def _gen_serve(task):
+    k, seed = task
+    _, w, h, fmt, gen, _ = SERVE_KINDS[k]
+    return S.make_frame(w, h, fmt, seed=seed, **gen)
+
+
+def serve_requests(n, seed=4000):
+    """(stream, kind, algo, bm) per request; bm on 10 % of them."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(SERVE_STREAMS)), int(rng.integers(len(SERVE_KINDS))),
+             int(rng.choice([2, 4, 6])), bool(rng.random() < 0.1)) for _ in range(n)]
+
+
+def serving_leg(frames, n_requests, lanes=4, max_batch=8, budget=8 << 30):
+    """Poisson arrivals at 1.2x the per-frame path's capacity into the
+    continuous-batching server; latency from submit to completion on the
+    server's clock."""
+    import numpy as np
+    import torch
+    import lgcr
+
+    def pinned_like(a):
+        t = torch.empty(a.shape, dtype={np.uint8: torch.uint8, np.uint16: torch.int16,
+                                        np.float32: torch.float32}[a.dtype.type], pin_memory=True)
+        v = t.numpy()
+        return v.view(a.dtype) if a.dtype == np.uint16 else v
+
+    pins = {}
+    for (k, s), planes in frames.items():
+        pp = [pinned_like(p) for p in planes]
+        for d, src in zip(pp, planes):
+            d[...] = src
+        pins[(k, s)] = pp
+    filters, rings, ring_next = {}, {}, {}
+    reqs = serve_requests(n_requests)
+
+    def filt(k, algo, bm):
+        key = (k, algo, bm)
+        if key not in filters:
+            _, w, h, fmt, _, fa = SERVE_KINDS[k]
+            filters[key] = lgcr.Recon(lgcr.format_of(frames[(k, 0)], None if fmt.is_float else fmt.bits),
+                                      algo=algo, bm=int(bm), **fa)
+        return filters[key]
+
+    def out_set(k):
+        if k not in rings:
+            f = filt(k, 2, False)
+            same = f.out_w == SERVE_KINDS[k][1] and f.out_h == SERVE_KINDS[k][2]
+            rings[k] = [[None if (p == 0 and same) else pinned_like(np.empty((f.out_h, f.out_w), f.dtype))
+                         for p in range(3)] for _ in range(SERVE_RING)]
+            ring_next[k] = 0
+        i = ring_next[k]
+        ring_next[k] = (i + 1) % SERVE_RING
+        return i, rings[k][i]
+
+    # warm-up: tables and workspaces of every filter the stream uses
+    for (_, k, algo, bm) in {(0, k, a, b) for (_, k, a, b) in reqs}:
+        filt(k, algo, bm).frame(pins[(k, 0)], -1, out=out_set(k)[1])
+    # capacity of the per-frame path (one calling thread) on the stream's mix
+    sample = reqs[:min(100, len(reqs))]
+    t0 = time.perf_counter()
+    for (s, k, algo, bm) in sample:
+        filt(k, algo, bm).frame(pins[(k, s % SERVE_SEEDS)], -1, out=out_set(k)[1])
+    plain_fps = len(sample) / (time.perf_counter() - t0)
+    rate = 1.2 * plain_fps
+    arrivals = np.cumsum(np.random.default_rng(4001).exponential(1.0 / rate, len(reqs)))
+    server = lgcr.Server(budget_bytes=budget, max_batch=max_batch, lanes=lanes,
+                         queue_capacity=len(reqs) + 1)
+    tickets = [None] * len(reqs)
+    owner = {}                     # (kind, ring slot) -> request index using it
+    infos = [None] * len(reqs)
+    pixels = 0
+    start = time.perf_counter()
+    for i, (s, k, algo, bm) in enumerate(reqs):
+        delay = start + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        slot, out = out_set(k)
+        prev = owner.get((k, slot))
+        if prev is not None and infos[prev] is None:
+            infos[prev] = server.wait(tickets[prev])[1]      # ring slot still in flight
+        owner[(k, slot)] = i
+        f = filt(k, algo, bm)
+        tickets[i] = server.submit(f, pins[(k, s % SERVE_SEEDS)], out)
+        if tickets[i] < 0:
+            raise RuntimeError(f"serving submit failed: {tickets[i]}")
+        pixels += f.out_w * f.out_h
+    for i in range(len(reqs)):
+        if infos[i] is None:
+            infos[i] = server.wait(tickets[i])[1]
+    server.close()
+    lat = np.array([inf.done_ms - inf.submit_ms for inf in infos])
+    span_ms = max(inf.done_ms for inf in infos) - min(inf.submit_ms for inf in infos)
+    bad = sum(1 for inf in infos if inf.status != 0)
+    return {
+        "requests": len(reqs), "failed": bad, "streams": SERVE_STREAMS,
+        "kinds": [kd[0] for kd in SERVE_KINDS], "algos": [2, 4, 6], "bm_fraction": 0.1,
+        "content": f"{SERVE_SEEDS} seeded frames per kind shared by the streams",
+        "per_frame_capacity_fps": round(plain_fps, 1), "arrival_rate_fps": round(rate, 1),
+        "throughput_fps": round(len(reqs) / (span_ms / 1000), 1),
+        "throughput_mpix_s": round(pixels / (span_ms / 1000) / 1e6, 1),
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                       "p99": round(float(np.percentile(lat, 99)), 3),
+                       "p99.9": round(float(np.percentile(lat, 99.9)), 3)},
+        "server": {"lanes": lanes, "max_batch": max_batch, "budget_gb": budget / 2 ** 30},
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -472,6 +601,12 @@ def our_arm(args):
         "roofline": rl,
         "clocks": clk.summary(),
     }
+    if rank == 0 and args.serve_requests > 0:
+        # content of the serving stream (spawned workers: safe after CUDA init)
+        keys = [(k, s) for k in range(len(SERVE_KINDS)) for s in range(SERVE_SEEDS)]
+        with mp.get_context("spawn").Pool(min(len(keys), max(1, (os.cpu_count() or 2) - 1), 16)) as pool:
+            made = pool.map(_gen_serve, [(k, 7000 + 97 * k + s) for k, s in keys])
+        result["serving"] = serving_leg(dict(zip(keys, made)), args.serve_requests, lanes=args.serve_lanes)
     if rank == 0 and cpu_frames is not None:
         threads = cpu_threads()
         value_cpu, total_s, times = run_cpu(cpu_frames, specs, 1, 0, threads, threads,
@@ -503,6 +638,10 @@ def main():
     ap.add_argument("--e2e-threads", type=int, default=0,
                     help="host threads calling the per-frame C ABI in the e2e leg (frames in "
                          "flight); default: the host's cores, at most 16, as the reference arm")
+    ap.add_argument("--serve-requests", type=int, default=4000,
+                    help="requests of the serving leg (0 skips it)")
+    ap.add_argument("--serve-lanes", type=int, default=4,
+                    help="concurrent device batches of the serving leg")
     ap.add_argument("--batch-only", action="store_true",
                     help="time the batched form only (profiler captures)")
     args = ap.parse_args()

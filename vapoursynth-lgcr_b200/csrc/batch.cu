@@ -17,7 +17,6 @@ struct StageEvent {
 };
 
 struct lgcr_batch {
-    std::vector<std::unique_ptr<Workspace>> slots;
     int capacity = 0;
     FrameJob *dJobs = nullptr, *hJobs = nullptr;
     int *dPrefix = nullptr, *hPrefix = nullptr;
@@ -150,13 +149,22 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
     // the pinned descriptors are rewritten: the previous run must have read them
     if (b->pending)
         cudaEventSynchronize(b->done);
-    if ((int)b->slots.size() < count)
-        b->slots.resize(count);
+    // workspaces come from each frame's filter pool and go back after the
+    // launch: a mixed stream keeps them resident across batches instead of
+    // reallocating whenever a slot's filter changes
+    std::vector<Workspace *> taken;
+    taken.reserve(count);
+    auto giveBack = [&]() {
+        for (Workspace *ws : taken)
+            ws->owner->release(ws);
+        taken.clear();
+    };
     std::vector<FrameJob> jobs(count);
     std::string sig = std::to_string(count);
     for (int i = 0; i < count; ++i) {
         const lgcr_batch_item &it = items[i];
         if (!it.filter) {
+            giveBack();
             setError("LGCR: batch item without filter");
             return LGCR_E_ARGUMENT;
         }
@@ -166,18 +174,23 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
         t.p = F->sited(it.chroma_location);
         t.tables = F->tablesFor(t.p.shiftX, t.p.shiftY);
         if (!t.tables) {
+            giveBack();
             setError("LGCR: failed to upload geometry tables");
             return LGCR_E_NOMEM;
         }
-        if (!b->slots[i] || b->slots[i]->owner != F) {
-            b->slots[i] = F->makeWorkspace(false);
-            if (!b->slots[i]) {
-                setError("LGCR: device workspace allocation failed");
-                return LGCR_E_NOMEM;
-            }
-            b->signature.clear();
+        Workspace *ws = F->acquire(false);
+        if (!ws) {
+            giveBack();
+            setError("LGCR: device workspace allocation failed");
+            return LGCR_E_NOMEM;
         }
-        t.ws = b->slots[i].get();
+        if (ws->used && cudaStreamWaitEvent(s, ws->done, 0) != cudaSuccess) {
+            F->release(ws);
+            giveBack();
+            return cudaFail(cudaGetLastError(), "lgcr_batch_run");
+        }
+        taken.push_back(ws);
+        t.ws = ws;
         for (int p = 0; p < 3; ++p) {
             t.in[p] = it.in[p];
             t.out[p] = it.out[p];
@@ -197,31 +210,46 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
         if (!b->exec || b->signature != sig) {
             if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
             cudaGraph_t graph = nullptr;
-            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                giveBack();
                 return cudaFail(cudaGetLastError(), "graph capture");
+            }
             launches = enqueue(b, jobs, plan, s, true);
             const cudaError_t e = cudaStreamEndCapture(s, &graph);
-            if (e != cudaSuccess || launches < 0)
+            if (e != cudaSuccess || launches < 0) {
+                giveBack();
                 return cudaFail(e != cudaSuccess ? e : cudaGetLastError(), "graph capture");
+            }
             const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
             cudaGraphDestroy(graph);
-            if (ie != cudaSuccess)
+            if (ie != cudaSuccess) {
+                giveBack();
                 return cudaFail(ie, "graph instantiate");
+            }
             b->signature = sig;
             b->lastLaunches = launches;
         }
         const cudaError_t e = cudaGraphLaunch(b->exec, s);
-        if (e != cudaSuccess)
+        if (e != cudaSuccess) {
+            giveBack();
             return cudaFail(e, "graph launch");
+        }
         launches = b->lastLaunches;
     } else {
         launches = enqueue(b, jobs, plan, s, true);
-        if (launches < 0)
+        if (launches < 0) {
+            giveBack();
             return cudaFail(cudaGetLastError(), "lgcr_batch_run");
+        }
         b->lastLaunches = launches;
     }
     cudaEventRecord(b->done, s);
     b->pending = true;
+    for (Workspace *ws : taken) {
+        cudaEventRecord(ws->done, s);
+        ws->used = true;
+    }
+    giveBack();
     return LGCR_OK;
 }
 

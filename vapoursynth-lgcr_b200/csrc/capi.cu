@@ -30,15 +30,6 @@ cudaStream_t threadStream() {
     return s;
 }
 
-// Plane copy between host and device: one linear copy when both sides are
-// packed (pitch == row bytes), else a 2D copy.
-cudaError_t copyPlane(void *dst, size_t dpitch, const void *src, size_t spitch, size_t rowBytes,
-                      size_t rows, cudaMemcpyKind kind, cudaStream_t s) {
-    if (dpitch == rowBytes && spitch == rowBytes)
-        return cudaMemcpyAsync(dst, src, rowBytes * rows, kind, s);
-    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, rowBytes, rows, kind, s);
-}
-
 bool checkPlane(const lgcr_plane &p, int w, int h, int bps, bool allowNull) {
     if (!p.data)
         return allowNull;

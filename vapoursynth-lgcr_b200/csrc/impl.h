@@ -107,6 +107,7 @@ struct Workspace {
     size_t stageInPitch[3] = {0, 0, 0}, stageOutPitch[3] = {0, 0, 0};
     cudaEvent_t done = nullptr;
     bool used = false;
+    bool hostStaging = false;           // has the host-buffer staging planes
     ~Workspace();
 };
 
@@ -125,12 +126,15 @@ struct Filter {
     float *dLut = nullptr;
     std::mutex mu;
     std::vector<std::unique_ptr<DeviceTables>> tables;
-    std::vector<std::unique_ptr<Workspace>> idle;
-    std::atomic<int> live{0};
+    std::vector<std::unique_ptr<Workspace>> idle, idleBatch;   // per-frame / batched forms
+    std::atomic<int> live{0}, liveBatch{0};
     ~Filter();
 
     const DeviceTables *tablesFor(double shiftX, double shiftY);
-    Workspace *acquire();
+    // A workspace from the filter's pool (per-frame form: with host staging;
+    // batched/serving forms: without). The caller must order its work after
+    // the workspace's previous frame (event `done`) when `used` is set.
+    Workspace *acquire(bool hostStaging = true);
     void release(Workspace *ws);
     std::unique_ptr<Workspace> makeWorkspace(bool hostStaging);
     size_t workspaceBytes();
@@ -170,6 +174,15 @@ void setStageShape(int stage, int bx, int by);
 int guidedVariant();
 void setGuidedVariant(int variant);
 const char *setError(const std::string &msg);
+
+// Plane copy between host and device: one linear copy when both sides are
+// packed (pitch == row bytes), else a 2D copy.
+inline cudaError_t copyPlane(void *dst, size_t dpitch, const void *src, size_t spitch,
+                             size_t rowBytes, size_t rows, cudaMemcpyKind kind, cudaStream_t s) {
+    if (dpitch == rowBytes && spitch == rowBytes)
+        return cudaMemcpyAsync(dst, src, rowBytes * rows, kind, s);
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, rowBytes, rows, kind, s);
+}
 int cudaFail(cudaError_t e, const char *where);
 
 } // namespace lgcr_b200

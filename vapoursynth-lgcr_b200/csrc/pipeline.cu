@@ -548,27 +548,31 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
 
 // Prefer an idle workspace whose last frame has finished on the device; grow
 // the pool (up to a few per filter) rather than wait for one in flight.
-Workspace *Filter::acquire() {
+Workspace *Filter::acquire(bool hostStaging) {
     constexpr int kMaxWorkspaces = 4;
+    auto &pool = hostStaging ? idle : idleBatch;
+    auto &count = hostStaging ? live : liveBatch;
     {
         std::lock_guard<std::mutex> lock(mu);
-        for (size_t i = 0; i < idle.size(); ++i) {
-            Workspace *ws = idle[i].get();
+        for (size_t i = 0; i < pool.size(); ++i) {
+            Workspace *ws = pool[i].get();
             if (!ws->used || cudaEventQuery(ws->done) == cudaSuccess) {
-                idle[i].release();
-                idle.erase(idle.begin() + i);
+                pool[i].release();
+                pool.erase(pool.begin() + i);
                 return ws;
             }
         }
-        if (live.load() >= kMaxWorkspaces && !idle.empty()) {
-            Workspace *ws = idle.front().release();
-            idle.erase(idle.begin());
-            return ws;   // caller waits for its event
+        if (count.load() >= kMaxWorkspaces && !pool.empty()) {
+            Workspace *ws = pool.front().release();
+            pool.erase(pool.begin());
+            return ws;   // caller orders its work after the event
         }
     }
-    auto ws = makeWorkspace(true);
-    if (ws)
-        live.fetch_add(1);
+    auto ws = makeWorkspace(hostStaging);
+    if (ws) {
+        ws->hostStaging = hostStaging;
+        count.fetch_add(1);
+    }
     return ws.release();
 }
 
@@ -576,7 +580,7 @@ void Filter::release(Workspace *ws) {
     if (!ws)
         return;
     std::lock_guard<std::mutex> lock(mu);
-    idle.emplace_back(ws);
+    (ws->hostStaging ? idle : idleBatch).emplace_back(ws);
 }
 
 // ---------------------------------------------------------------------------

@@ -156,8 +156,8 @@ void laneLoop(lgcr_server *S, int laneIndex) {
             for (int p = 0; p < 3; ++p) {
                 const size_t inRow = size_t(r->in[p].width) * bps;
                 if (!slots[i]->ensure(p, true, inRow * r->in[p].height)) { status = LGCR_E_NOMEM; break; }
-                if (cudaMemcpy2DAsync(slots[i]->in[p], inRow, r->in[p].data, r->in[p].stride, inRow,
-                                      r->in[p].height, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+                if (copyPlane(slots[i]->in[p], inRow, r->in[p].data, r->in[p].stride, inRow,
+                              r->in[p].height, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
                     status = LGCR_E_CUDA; break;
                 }
                 items[i].in[p] = { slots[i]->in[p], (ptrdiff_t)inRow, r->in[p].width, r->in[p].height };
@@ -179,8 +179,8 @@ void laneLoop(lgcr_server *S, int laneIndex) {
                 if (!r->out[p].data)
                     continue;
                 const size_t outRow = size_t(r->out[p].width) * bps;
-                if (cudaMemcpy2DAsync(r->out[p].data, r->out[p].stride, slots[i]->out[p], outRow, outRow,
-                                      r->out[p].height, cudaMemcpyDeviceToHost, stream) != cudaSuccess) {
+                if (copyPlane(r->out[p].data, r->out[p].stride, slots[i]->out[p], outRow, outRow,
+                              r->out[p].height, cudaMemcpyDeviceToHost, stream) != cudaSuccess) {
                     status = LGCR_E_CUDA; break;
                 }
             }
