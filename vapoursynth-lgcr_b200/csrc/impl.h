@@ -95,6 +95,7 @@ struct Workspace {
     unsigned long long *counters = nullptr;
     double *uvd = nullptr;
     float *hTab = nullptr;
+    float *wExt = nullptr;              // W x H float4 hull plane, then W x H float2 luma plane
     uint32_t *actList = nullptr;
     float *aff = nullptr, *yc1 = nullptr, *yc2 = nullptr, *ycTmp = nullptr;
     float *detail = nullptr, *detailTmp = nullptr, *detailTmp2 = nullptr, *dTab = nullptr;

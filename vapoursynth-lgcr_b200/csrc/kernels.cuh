@@ -11,9 +11,15 @@ namespace lgcr_b200 {
 
 // k_plain: output rows per block (32 columns wide, 32x8 threads) and the
 // most horizontal-table rows one block stages in shared memory.
-constexpr int kPlainRows = 64;          // tall blocks (frames whose windows fit)
+constexpr int kPlainRows = 64;          // tallest blocks (frames whose windows fit)
 constexpr int kPlainRowsShort = 32;     // other frames
 constexpr int kPlainStagedRows = 40;
+// k_plain's staged rows (float sums, hull float4, luma extrema float2 per
+// row and column: 32 B) in dynamic shared memory; with the static row
+// tables a block stays under 48 KB, so four blocks per SM keep 60 KB of L1.
+constexpr size_t kPlainDynSmem = size_t(kPlainStagedRows) * 32 * (8 + 16 + 8);
+// k_detail_map: most horizontal-table rows one block stages.
+constexpr int kDetailStagedRows = 40;
 
 // k_convert: samples per warp (one row segment) and warps per block; the
 // luma blocks of a frame come first, then the chroma blocks.

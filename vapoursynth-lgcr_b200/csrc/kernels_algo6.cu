@@ -353,8 +353,8 @@ __device__ __forceinline__ double detailVertical(const DetailRows &R, const doub
 
 __global__ void __launch_bounds__(256)
 k_detail_map(LGCR_STAGE_ARGS) {
-    __shared__ double sH[kPlainStagedRows][32];
-    __shared__ float2 sE[kPlainStagedRows][32];
+    __shared__ double sH[kDetailStagedRows][32];
+    __shared__ float2 sE[kDetailStagedRows][32];
     __shared__ float sD[kDetailRowsTall + 2][33];
     __shared__ float sX[kDetailRowsTall + 2][33];
     __shared__ DetailRows R;

@@ -223,10 +223,10 @@ __device__ __forceinline__ void emit(const FrameJob &J, int ox, int oy, float u,
 
 // Vertical pass over table rows staged in shared memory: same arithmetic and
 // order as plainFromTableT, rows indexed relative to the staged block. The
-// horizontal sums are staged already widened to double (the float-rounded
-// ring value, as the reference multiplies it in double).
+// horizontal sums are staged as the float-rounded ring value and widened to
+// double (exact) where the reference multiplies them in double.
 template <int SUP>
-__device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2 (*sHV)[32],
+__device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 (*sHV)[32],
                                                 const float4 (*sE)[32], int syLo, int lx, int ox,
                                                 int oy, float &outU, float &outV) {
     const AxisView &ax = J.ax, &ay = J.ay;
@@ -241,11 +241,11 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const double2
         if (__ldg(amy + j) == 0)
             continue;
         const int r = (J.noClampY ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
-        const double2 h = sHV[r][lx];
+        const float2 h = sHV[r][lx];
         const float4 e = sE[r][lx];
         const double w = __ldg(wy + j);
-        vU = fma(w, h.x, vU);
-        vV = fma(w, h.y, vV);
+        vU = fma(w, (double)h.x, vU);
+        vV = fma(w, (double)h.y, vV);
         mnU = runMin(mnU, e.x); mxU = runMax(mxU, e.y);
         mnV = runMin(mnV, e.z); mxV = runMax(mxV, e.w);
     }
@@ -280,7 +280,7 @@ struct PlainRows {
 // The same vertical pass with the row data from PlainRows and the column
 // data (wsX, waX, posX) held in registers.
 template <int SUP, bool NOCLAMP>
-__device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (*sHV)[32],
+__device__ __forceinline__ void plainFromRows(const FrameJob &J, const float2 (*sHV)[32],
                                               const float4 (*sE)[32], const PlainRows &R, int k,
                                               int syLo, int lx, float wsX, float waX, float posX,
                                               float &outU, float &outV) {
@@ -293,11 +293,11 @@ __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (
         if (!((act >> j) & 1u))
             continue;
         const int r = (NOCLAMP ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
-        const double2 h = sHV[r][lx];
+        const float2 h = sHV[r][lx];
         const float4 e = sE[r][lx];
         const double w = R.w[k][j];
-        vU = fma(w, h.x, vU);
-        vV = fma(w, h.y, vV);
+        vU = fma(w, (double)h.x, vU);
+        vV = fma(w, (double)h.y, vV);
         mnU = runMin(mnU, e.x); mxU = runMax(mxU, e.y);
         mnV = runMin(mnV, e.z); mxV = runMax(mxV, e.w);
     }
@@ -318,15 +318,26 @@ __device__ __forceinline__ void plainFromRows(const FrameJob &J, const double2 (
     outV = (float)vV;
 }
 
+// Shared-memory rows of one k_plain block: float-rounded horizontal sums
+// (widened to double where the vertical pass multiplies them), chroma hull and (frames whose guided pass reads the folded extrema) luma
+// extrema of each staged (chroma row, output column).
+struct PlainStage {
+    float2 (*hv)[32];
+    float4 (*e)[32];
+    float2 (*l)[32];
+};
+
 // Horizontal entries of the rows [syLo, syLo + nRows) for output column ox
 // into shared memory; table rows this block owns (sy < syOwnEnd) also go to
 // the frame's horizontal table for the guided pass. Two rows per step keep
 // both rows' loads in flight together.
 __device__ __forceinline__ void putEntry(const FrameJob &J, int ox, int lx, int r, int sy, const float4 &a,
                                          const float4 &b, int syOwnEnd, bool writeTable,
-                                         double2 (*sHV)[32], float4 (*sE)[32]) {
-    sHV[r][lx] = make_double2((double)a.x, (double)a.y);
-    sE[r][lx] = make_float4(a.z, a.w, b.x, b.y);
+                                         const PlainStage &s) {
+    s.hv[r][lx] = make_float2(a.x, a.y);
+    s.e[r][lx] = make_float4(a.z, a.w, b.x, b.y);
+    if (J.wLum)
+        s.l[r][lx] = make_float2(b.z, b.w);
     if (writeTable && sy < syOwnEnd)
         storeEntry(J, ox, sy, a, b);
 }
@@ -334,43 +345,67 @@ __device__ __forceinline__ void putEntry(const FrameJob &J, int ox, int lx, int 
 template <int SUP, bool NOCLAMP>
 __device__ __forceinline__ void stageRowsT(const FrameJob &J, const HColumn<SUP> &col, int ox, int lx,
                                            int syLo, int nRows, int syOwnEnd, bool writeTable,
-                                           double2 (*sHV)[32], float4 (*sE)[32]) {
+                                           const PlainStage &s) {
     const int step = blockDim.y;
     int r = threadIdx.y;
     for (; r + step < nRows; r += 2 * step) {
         float4 a0, b0, a1, b1;
         hEntry<SUP, NOCLAMP>(J, col, syLo + r, a0, b0);
         hEntry<SUP, NOCLAMP>(J, col, syLo + r + step, a1, b1);
-        putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, sHV, sE);
-        putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, sHV, sE);
+        putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, s);
+        putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, s);
     }
     if (r < nRows) {
         float4 a, b;
         hEntry<SUP, NOCLAMP>(J, col, syLo + r, a, b);
-        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sE);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, s);
     }
 }
 
 template <int SUP>
 __device__ __forceinline__ void stageRows(const FrameJob &J, int ox, int lx, int syLo, int nRows,
-                                          int syOwnEnd, bool writeTable, double2 (*sHV)[32],
-                                          float4 (*sE)[32]) {
+                                          int syOwnEnd, bool writeTable, const PlainStage &s) {
     HColumn<SUP> col;
     col.load(J.ax, ox);
     if (J.noClampX)
-        stageRowsT<SUP, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE);
+        stageRowsT<SUP, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
     else
-        stageRowsT<SUP, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE);
+        stageRowsT<SUP, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
 }
 
 __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int lx, int syLo, int nRows,
-                                                 int syOwnEnd, bool writeTable, double2 (*sHV)[32],
-                                                 float4 (*sE)[32]) {
+                                                 int syOwnEnd, bool writeTable, const PlainStage &s) {
     for (int r = threadIdx.y; r < nRows; r += blockDim.y) {
         float4 a, b;
         hEntryGeneric(J, ox, syLo + r, a, b);
-        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, sHV, sE);
+        putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, s);
     }
+}
+
+// Extrema of a listed pixel's guided window (pass 1 of reconstructChromaImpl,
+// src/recon.cpp:258-367: the chroma hull and the luma range over the active
+// taps) folded from the staged rows in the same row order as the guided
+// pass's own fold, to the frame's extrema planes.
+template <int SUP, bool NOCLAMP>
+__device__ __forceinline__ void extremaFromRows(const FrameJob &J, const float4 (*sE)[32],
+                                                const float2 (*sL)[32], const PlainRows &R, int k,
+                                                int syLo, int lx, size_t o) {
+    const int ty0 = R.ty0[k];
+    const uint32_t act = R.act[k];
+    float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f, mnL = 1e30f, mxL = -1e30f;
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((act >> j) & 1u))
+            continue;
+        const int r = (NOCLAMP ? ty0 + j : iclamp(ty0 + j, 0, J.ch - 1)) - syLo;
+        const float4 e = sE[r][lx];
+        const float2 l = sL[r][lx];
+        mnU = runMin(mnU, e.x); mxU = runMax(mxU, e.y);
+        mnV = runMin(mnV, e.z); mxV = runMax(mxV, e.w);
+        mnL = runMin(mnL, l.x); mxL = runMax(mxL, l.y);
+    }
+    J.wHull[o] = make_float4(mnU, mxU, mnV, mxV);
+    J.wLum[o] = make_float2(mnL, mxL);
 }
 
 // Plain stage: every pixel the guided pass does not finalize. A block covers
@@ -387,8 +422,12 @@ __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int 
 // and active-pixel bits staged once per block for supports up to 8.
 __global__ void __launch_bounds__(256, 4)
 k_plain(LGCR_STAGE_ARGS) {
-    __shared__ double2 sHV[kPlainStagedRows][32];
-    __shared__ float4 sE[kPlainStagedRows][32];      // mnU mxU mnV mxV
+    extern __shared__ __align__(16) unsigned char plainRowsSmem[];
+    float2 (*sHV)[32] = reinterpret_cast<float2 (*)[32]>(plainRowsSmem);
+    float4 (*sE)[32] = reinterpret_cast<float4 (*)[32]>(      // mnU mxU mnV mxV
+        plainRowsSmem + size_t(kPlainStagedRows) * 32 * 8);
+    float2 (*sL)[32] = reinterpret_cast<float2 (*)[32]>(      // mnL mxL
+        plainRowsSmem + size_t(kPlainStagedRows) * 32 * 24);
     __shared__ PlainRows R;
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -431,9 +470,12 @@ k_plain(LGCR_STAGE_ARGS) {
             R.pos[tid] = __ldg(J.ay.pos + oy);
         }
     }
-    // active-pixel bits: listed pixels are skipped here; algo 6 pixels the
-    // detail transfer leaves alone are stored final here
-    const bool maskWords = (skipListed || J.finalInTransfer) && J.sparse && J.sameSize;
+    // active-pixel bits: listed pixels are skipped here (after folding their
+    // guided windows' extrema); algo 6 pixels the detail transfer leaves
+    // alone are stored final here
+    const bool foldExtrema = J.wHull != nullptr;    // implies fused row tables
+    const bool needAct = skipListed || J.finalInTransfer || foldExtrema;
+    const bool maskWords = needAct && J.sparse && J.sameSize;
     if (maskWords && tid < rowsHere)
         R.maskWord[tid] = __ldg(J.mask + (size_t)(oy0 + tid) * J.maskWords + (colBase >> 5));
     if (fused) {
@@ -441,12 +483,13 @@ k_plain(LGCR_STAGE_ARGS) {
         const int syOwnEnd = (oy0 + J.plainRows < J.H)
             ? iclamp(__ldg(J.ay.start + oy0 + J.plainRows), 0, J.ch - 1) : J.ch;
         const bool writeTable = J.listed && J.hTab;
+        const PlainStage s{sHV, sE, sL};
         if (ox < J.W) {
             switch (J.ax.sup) {
-            case 4: stageRows<4>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
-            case 6: stageRows<6>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
-            case 8: stageRows<8>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
-            default: stageRowsGeneric(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, sHV, sE); break;
+            case 4: stageRows<4>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, s); break;
+            case 6: stageRows<6>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, s); break;
+            case 8: stageRows<8>(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, s); break;
+            default: stageRowsGeneric(J, ox, lx, syLo, nRows, syOwnEnd, writeTable, s); break;
             }
         }
     } else if (staged && ox < J.W) {
@@ -454,7 +497,7 @@ k_plain(LGCR_STAGE_ARGS) {
             const float4 *h =
                 reinterpret_cast<const float4 *>(J.hTab + ((size_t)(syLo + r) * J.W + ox) * 8);
             const float4 a = __ldg(h), b = __ldg(h + 1);
-            sHV[r][lx] = make_double2((double)a.x, (double)a.y);
+            sHV[r][lx] = make_float2(a.x, a.y);
             sE[r][lx] = make_float4(a.z, a.w, b.x, b.y);
         }
     }
@@ -471,8 +514,24 @@ k_plain(LGCR_STAGE_ARGS) {
         const int oy = oy0 + k;
         // listed pixels of algo 2 and integer algo 4 are written by k_guided
         bool act = false;
-        if (skipListed || J.finalInTransfer) {
+        if (needAct) {
             act = maskWords ? ((R.maskWord[k] >> lx) & 1u) != 0 : pixelActive(J, ox, oy);
+            if (act && foldExtrema) {
+                const size_t o = (size_t)oy * J.W + ox;
+                if (J.noClampY) {
+                    switch (sup) {
+                    case 4: extremaFromRows<4, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                    case 6: extremaFromRows<6, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                    default: extremaFromRows<8, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                    }
+                } else {
+                    switch (sup) {
+                    case 4: extremaFromRows<4, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                    case 6: extremaFromRows<6, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                    default: extremaFromRows<8, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                    }
+                }
+            }
             if (act && skipListed)
                 continue;
         }
@@ -693,6 +752,14 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     const AxisView &ax = J.ax, &ay = J.ay;
     const int sw = J.sw, sh = J.sh, cw = J.cw, ch = J.ch;
     Guided g;
+    // window extrema folded by k_plain (issued first: nothing else waits on them)
+    float4 wHull = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float2 wLum = make_float2(0.0f, 0.0f);
+    if (J.wHull) {
+        const size_t o = (size_t)oy * J.W + ox;
+        wHull = __ldg(J.wHull + o);
+        wLum = __ldg(J.wLum + o);
+    }
     // guide metadata (prepareGuideRow, recon.cpp:155-220)
     const int bxi = __ldg(ax.lbI0 + ox), byi = __ldg(ay.lbI0 + oy);
     const float bxf = __ldg(ax.lbF + ox), byf = __ldg(ay.lbF + oy);
@@ -750,7 +817,11 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
     float maxAbsDL = 0.0f;
     float hMinU = 1e30f, hMaxU = -1e30f, hMinV = 1e30f, hMaxV = -1e30f;
-    if (!J.radial && J.hTab) {
+    if (J.wHull) {
+        hMinU = wHull.x; hMaxU = wHull.y; hMinV = wHull.z; hMaxV = wHull.w;
+        maxAbsDL = smax(maxAbsDL, fabsf(wLum.y - L0));
+        maxAbsDL = smax(maxAbsDL, fabsf(wLum.x - L0));
+    } else if (!J.radial && J.hTab) {
         float ext[6];
         switch (ay.sup) {
         case 4: windowExtrema<4>(J, ox, ty0, amy, ext); break;

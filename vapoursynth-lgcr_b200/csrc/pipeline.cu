@@ -349,7 +349,7 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         };
         t->detailRows = kDetailRowsTall;
         t->detailMaxRows = detailRowsRead(kDetailRowsTall);
-        if (t->detailMaxRows > kPlainStagedRows) {
+        if (t->detailMaxRows > kDetailStagedRows) {
             t->detailRows = kDetailTile;
             t->detailMaxRows = detailRowsRead(kDetailTile);
         }
@@ -410,11 +410,15 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         }
         return most;
     };
-    t->plainRows = kPlainRows;
-    t->plainMaxRows = plainRowsRead(kPlainRows);
-    if (t->plainMaxRows > kPlainStagedRows) {
-        t->plainRows = kPlainRowsShort;
-        t->plainMaxRows = plainRowsRead(kPlainRowsShort);
+    t->plainRows = kPlainRowsShort;
+    t->plainMaxRows = plainRowsRead(kPlainRowsShort);
+    for (int rows = kPlainRows; rows > kPlainRowsShort; rows -= 8) {
+        const int most = plainRowsRead(rows);
+        if (most <= kPlainStagedRows) {
+            t->plainRows = rows;
+            t->plainMaxRows = most;
+            break;
+        }
     }
     if (p.k.radial)
         t->rad = radialView(t->arena, orad);
@@ -485,6 +489,7 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     Slot sCnt = take(kCntCount * sizeof(unsigned long long));
     const bool listed = guided && (p.algo == 2 || p.algo == 4);
     Slot sUvd = take(C * 16), sHTab = take(size_t(p.outW) * ch * 32, !p.k.radial);
+    Slot sWExt = take(O * 24, listed && !p.k.radial && p.k.kernel != Kernel::Bilinear);
     Slot sList = take(O * 4, listed);
     const bool algo6 = guided && p.algo == 6, algo4 = guided && p.algo == 4;
     Slot sAff = take(9 * C * 4, algo6), sYc1 = take(C * 4, algo6), sYc2 = take(C * 4, algo6);
@@ -523,6 +528,7 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     ws->counters = (unsigned long long *)ar.at(sCnt.off);
     ws->uvd = sUvd.on ? (double *)ar.at(sUvd.off) : nullptr;
     ws->hTab = F(sHTab);
+    ws->wExt = F(sWExt);
     ws->actList = sList.on ? (uint32_t *)ar.at(sList.off) : nullptr;
     ws->aff = F(sAff); ws->yc1 = F(sYc1); ws->yc2 = F(sYc2);
     ws->detailTmp = F(sDt1); ws->detailTmp2 = F(sDt2); ws->detail = F(sDet); ws->dTab = F(sDTab);
@@ -693,6 +699,17 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     }
     J.plainFused = (J.hTab && !J.radial && T.plainMaxRows <= kPlainStagedRows) ? 1 : 0;
     J.plainRows = J.plainFused ? T.plainRows : kPlainRowsShort;
+    J.wHull = nullptr;
+    J.wLum = nullptr;
+    if (ws.wExt && J.listed && J.plainFused && J.kernel != 0 && T.aySup <= 8) {
+        // k_plain folds the guided windows' extrema for the listed pixels from
+        // its staged rows; the horizontal table is then only needed for the
+        // integer algo 4 plain base the guided pass recomputes
+        J.wHull = reinterpret_cast<float4 *>(ws.wExt);
+        J.wLum = reinterpret_cast<float2 *>(ws.wExt + size_t(J.W) * J.H * 4);
+        if (!(p.algo == 4 && J.outKind != kF32))
+            J.hTab = nullptr;
+    }
     {
         // every tap index in range: starts lie in [0, srcChromaN - sup] and the
         // integer-ratio chroma count equals the plane size
@@ -721,7 +738,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         J.ycTiled = (T.ycMaxSup <= 8 && T.ycMaxRows <= kYcRows) ? 1 : 0;
         J.detailRows = T.detailRows;
         J.detailFused = (J.dTab && !J.radial && J.kernel != 0 && T.sAxSup <= 8 && T.sAySup <= 8 &&
-                         T.detailMaxRows <= kPlainStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
+                         T.detailMaxRows <= kDetailStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
     }
     // algo 4
     J.lgf = ws.lgf;
@@ -928,7 +945,19 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_GATE, k_gate, b32x8);
     go(S_LGF_DENSE, k_lgf, b32x8);
     go(S_HPASS, k_hpass, b32x8);
-    go(S_PLAIN, k_plain, b32x8);
+    if (plan.totals[S_PLAIN] > 0) {
+        // the dynamic shared-memory opt-in is per device (idempotent, so a
+        // race between host threads only repeats it)
+        static std::atomic<int> plainOptIn[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !plainOptIn[dev].load()) {
+            cudaFuncSetAttribute(k_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPlainDynSmem));
+            if (dev >= 0 && dev < 64)
+                plainOptIn[dev].store(1);
+        }
+    }
+    go(S_PLAIN, k_plain, b32x8, kPlainDynSmem);
     if (plan.totals[S_GUIDED] > 0) {
         // persistent grid: enough resident blocks to fill every SM
         const int variant = guidedVariant();

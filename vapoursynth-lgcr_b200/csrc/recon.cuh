@@ -110,6 +110,8 @@ struct __align__(16) FrameJob {
     float *lumaTmp;                    // W x sh luma resize intermediate
     unsigned long long *counters;      // kCntCount
     float *hTab;                       // W x ch x 8: horizontal sums + window extrema
+    float4 *wHull;                     // W x H guided window chroma hull (mnU mxU mnV mxV)
+    float2 *wLum;                      // W x H guided window luma extrema (mnL mxL)
     double *uvd;                       // cw x ch x 2: (u, v) in FP64
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
