@@ -543,13 +543,20 @@ k_count(LGCR_STAGE_ARGS) {
 constexpr int GT_X = 32, GT_Y = 8, GH = 4;
 constexpr int GW = GT_X + 2 * GH, GHh = GT_Y + 2 * GH;
 
-// Gradients of the three planes at one tile slot: (gx, gy) of lc and U in
-// one 16-byte word, of V in an 8-byte word, so a bilinear corner is two
-// shared-memory loads.
+// Gradients of the three planes at one tile slot: (gx, gy) of lc in an
+// 8-byte word and (gxU, gxV, gyU, gyV) in a 16-byte word, so a bilinear
+// corner is two shared-memory loads and the U and V arithmetic runs on
+// packed pairs straight from the loaded registers.
 struct GateTile {
-    float4 g01[GHh][GW];
-    float2 g2[GHh][GW];
+    float2 gl[GHh][GW];
+    float4 guv[GHh][GW];
 };
+
+// U and V of one corner projected on the normal: (gxU*nx + gyU*ny,
+// gxV*nx + gyV*ny), each lane rounded as the scalar expression.
+__device__ __forceinline__ f32x2 projectUV(const float4 &g, f32x2 nx2, f32x2 ny2) {
+    return add2(mul2(pk2(g.x, g.y), nx2), mul2(pk2(g.z, g.w), ny2));
+}
 
 // Gate of the active sample (x, y). INTERIOR: the tile and its halo lie
 // inside the plane, so sample slots need no clamping.
@@ -560,7 +567,7 @@ __device__ __forceinline__ float gateAt(const GateTile &T, int x, int y, int x0,
     float sxx = 0.0f, sxy = 0.0f, syy = 0.0f;
     for (int dy = -1; dy <= 1; ++dy)
         for (int dx = -1; dx <= 1; ++dx) {
-            const float4 g = T.g01[sy(y + dy)][sx(x + dx)];
+            const float2 g = T.gl[sy(y + dy)][sx(x + dx)];
             const float a = g.x, b = g.y;
             sxx += a * a; sxy += a * b; syy += b * b;
         }
@@ -569,7 +576,9 @@ __device__ __forceinline__ float gateAt(const GateTile &T, int x, int y, int x0,
         return 0.0f;
     const TensorDir dir = principalDirection(sxx, sxy, syy);
     const float nx = dir.nx, ny = dir.ny;
-    float sumY = 0, sqY = 0, momY = 0, sumC = 0, sqC = 0, momC = 0;
+    // moments of (gY, gC) as packed pairs: sum, sum of squares, k-weighted sum
+    const f32x2 nx2 = pk2(nx, nx), ny2 = pk2(ny, ny);
+    f32x2 sum2 = pk2(0.0f, 0.0f), sq2 = sum2, mom2 = sum2;
     for (int k = -3; k <= 3; ++k) {
         const float px = (float)x + (float)k * nx;
         const float py = (float)y + (float)k * ny;
@@ -578,29 +587,36 @@ __device__ __forceinline__ float gateAt(const GateTile &T, int x, int y, int x0,
         const int bx0 = sx(rawX), bx1 = sx(rawX + 1);
         const int by0 = sy(rawY), by1 = sy(rawY + 1);
         const float fx = px - fpx, fy = py - fpy;
-        const float4 A = T.g01[by0][bx0], B = T.g01[by0][bx1], C = T.g01[by1][bx0], D = T.g01[by1][bx1];
-        const float2 A2 = T.g2[by0][bx0], B2 = T.g2[by0][bx1], C2 = T.g2[by1][bx0], D2 = T.g2[by1][bx1];
-        float s[3];
+        const float2 A = T.gl[by0][bx0], B = T.gl[by0][bx1], C = T.gl[by1][bx0], D = T.gl[by1][bx1];
+        float sY;
         {
             const float a = A.x * nx + A.y * ny, b = B.x * nx + B.y * ny;
             const float c = C.x * nx + C.y * ny, d = D.x * nx + D.y * ny;
-            s[0] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+            sY = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
         }
+        f32x2 sUV;
         {
-            const float a = A.z * nx + A.w * ny, b = B.z * nx + B.w * ny;
-            const float c = C.z * nx + C.w * ny, d = D.z * nx + D.w * ny;
-            s[1] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
+            const f32x2 a = projectUV(T.guv[by0][bx0], nx2, ny2), b = projectUV(T.guv[by0][bx1], nx2, ny2);
+            const f32x2 c = projectUV(T.guv[by1][bx0], nx2, ny2), d = projectUV(T.guv[by1][bx1], nx2, ny2);
+            const f32x2 fx2 = pk2(fx, fx), fy2 = pk2(fy, fy);
+            // a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy per lane
+            sUV = add2(add2(add2(a, mul2(sub2(b, a), fx2)), mul2(sub2(c, a), fy2)),
+                       mul2(mul2(add2(sub2(sub2(a, b), c), d), fx2), fy2));
         }
-        {
-            const float a = A2.x * nx + A2.y * ny, b = B2.x * nx + B2.y * ny;
-            const float c = C2.x * nx + C2.y * ny, d = D2.x * nx + D2.y * ny;
-            s[2] = a + (b - a) * fx + (c - a) * fy + (a - b - c + d) * fx * fy;
-        }
-        const float gY = fabsf(s[0]);
-        const float gC = sqrtf(s[1] * s[1] + s[2] * s[2]);
-        sumY += gY; sqY += gY * gY; momY += (float)k * gY;
-        sumC += gC; sqC += gC * gC; momC += (float)k * gC;
+        float su, sv;
+        up2(sUV, su, sv);
+        const float gY = fabsf(sY);
+        const float gC = sqrtf(su * su + sv * sv);
+        const f32x2 g2 = pk2(gY, gC);
+        const float kf = (float)k;
+        sum2 = add2(sum2, g2);
+        sq2 = add2(sq2, mul2(g2, g2));
+        mom2 = add2(mom2, mul2(pk2(kf, kf), g2));
     }
+    float sumY, sumC, sqY, sqC, momY, momC;
+    up2(sum2, sumY, sumC);
+    up2(sq2, sqY, sqC);
+    up2(mom2, momY, momC);
     if (sumY < 1e-9f || sumC < 1e-9f)
         return 0.0f;
     const float partY = sumY * sumY / (sqY + 1e-12f);
@@ -651,8 +667,8 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
             g[2 * p] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
             g[2 * p + 1] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
         }
-        T.g01[r][c] = make_float4(g[0], g[1], g[2], g[3]);
-        T.g2[r][c] = make_float2(g[4], g[5]);
+        T.gl[r][c] = make_float2(g[0], g[1]);
+        T.guv[r][c] = make_float4(g[2], g[4], g[3], g[5]);
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
