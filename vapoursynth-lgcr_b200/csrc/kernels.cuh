@@ -44,6 +44,10 @@ constexpr int kDilPadWords = 8;
 // k_count: chroma mask bytes per block.
 constexpr int kCountChunk = 16384;
 
+// k_gate: chroma rows per block (32 columns wide, 32x8 threads, each thread
+// takes every eighth row).
+constexpr int kGateRows = 16;
+
 __global__ void k_convert(LGCR_STAGE_ARGS);
 __global__ void k_tensor(LGCR_STAGE_ARGS);
 __global__ void k_dilate_h(LGCR_STAGE_ARGS);

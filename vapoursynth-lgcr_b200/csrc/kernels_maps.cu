@@ -540,7 +540,7 @@ k_count(LGCR_STAGE_ARGS) {
 // dense Sobel rows; the sparse reference computes the same values wherever
 // an active sample can read them.
 // ---------------------------------------------------------------------------
-constexpr int GT_X = 32, GT_Y = 8, GH = 4;
+constexpr int GT_X = 32, GT_Y = kGateRows, GH = 4;
 constexpr int GW = GT_X + 2 * GH, GHh = GT_Y + 2 * GH;
 
 // Gradients of the three planes at one tile slot: (gx, gy) of lc in an
@@ -628,9 +628,10 @@ __device__ __forceinline__ float gateAt(const GateTile &T, int x, int y, int x0,
     return (tw * tw * (3.0f - 2.0f * tw)) * (tp * tp * (3.0f - 2.0f * tp));
 }
 
-__global__ void __launch_bounds__(GT_X * GT_Y)
+__global__ void __launch_bounds__(GT_X * 8)
 k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    __shared__ float src[3][GT_Y + 2 * GH + 2][GT_X + 2 * GH + 2];
+    constexpr int SW = GW + 2, SH = GHh + 2;     // lc, U, V with the Sobel ring
+    __shared__ float src[3][SH][SW];
     __shared__ GateTile T;
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -640,49 +641,56 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     const int w = J.cw, h = J.ch;
     const int tilesX = (w + GT_X - 1) / GT_X;
     const int x0 = (tile % tilesX) * GT_X, y0 = (tile / tilesX) * GT_Y;
-    const int tid = threadIdx.y * GT_X + threadIdx.x;
-    const int nthreads = GT_X * GT_Y;
-    const float *planes[3] = { J.lc, J.U, J.V };
-    constexpr int SW = GT_X + 2 * GH + 2, SH = GT_Y + 2 * GH + 2;
-    for (int i = tid; i < 3 * SW * SH; i += nthreads) {
-        const int p = i / (SW * SH), rem = i % (SW * SH);
-        const int r = rem / SW, c = rem % SW;
-        const int yy = iclamp(y0 - GH - 1 + r, 0, h - 1), xx = iclamp(x0 - GH - 1 + c, 0, w - 1);
-        src[p][r][c] = ldf(planes[p] + (size_t)yy * w + xx);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    // samples at clamped positions of the tile, its halo and the Sobel ring
+    const bool srcInterior = x0 >= GH + 1 && y0 >= GH + 1 && x0 + GT_X + GH + 1 <= w &&
+                             y0 + GT_Y + GH + 1 <= h;
+    for (int r = ty; r < SH; r += 8) {
+        const int yy = srcInterior ? y0 - GH - 1 + r : iclamp(y0 - GH - 1 + r, 0, h - 1);
+        for (int c = tx; c < SW; c += GT_X) {
+            const int xx = srcInterior ? x0 - GH - 1 + c : iclamp(x0 - GH - 1 + c, 0, w - 1);
+            const size_t o = (size_t)yy * w + xx;
+            src[0][r][c] = ldf(J.lc + o);
+            src[1][r][c] = ldf(J.U + o);
+            src[2][r][c] = ldf(J.V + o);
+        }
     }
     __syncthreads();
     // gradients at clamped positions of the tile and its halo (the dense
     // Sobel rows of the reference; the sparse reference computes the same
     // values wherever an active sample reads them)
-    for (int i = tid; i < GW * GHh; i += nthreads) {
-        const int r = i / GW, c = i % GW;
-        const int yy = iclamp(y0 - GH + r, 0, h - 1), xx = iclamp(x0 - GH + c, 0, w - 1);
-        const int sr = yy - y0 + GH + 1, sc = xx - x0 + GH + 1;
-        float g[6];
+    for (int r = ty; r < GHh; r += 8) {
+        const int sr = (srcInterior ? y0 - GH + r : iclamp(y0 - GH + r, 0, h - 1)) - y0 + GH + 1;
+        for (int c = tx; c < GW; c += GT_X) {
+            const int sc = (srcInterior ? x0 - GH + c : iclamp(x0 - GH + c, 0, w - 1)) - x0 + GH + 1;
+            float g[6];
 #pragma unroll
-        for (int p = 0; p < 3; ++p) {
-            const float tl = src[p][sr - 1][sc - 1], t = src[p][sr - 1][sc], tr = src[p][sr - 1][sc + 1];
-            const float l = src[p][sr][sc - 1], rr = src[p][sr][sc + 1];
-            const float bl = src[p][sr + 1][sc - 1], b = src[p][sr + 1][sc], br = src[p][sr + 1][sc + 1];
-            g[2 * p] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
-            g[2 * p + 1] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
+            for (int p = 0; p < 3; ++p) {
+                const float tl = src[p][sr - 1][sc - 1], t = src[p][sr - 1][sc], tr = src[p][sr - 1][sc + 1];
+                const float l = src[p][sr][sc - 1], rr = src[p][sr][sc + 1];
+                const float bl = src[p][sr + 1][sc - 1], b = src[p][sr + 1][sc], br = src[p][sr + 1][sc + 1];
+                g[2 * p] = (tr + 2.0f * rr + br - tl - 2.0f * l - bl) * 0.125f;
+                g[2 * p + 1] = (bl + 2.0f * b + br - tl - 2.0f * t - tr) * 0.125f;
+            }
+            T.gl[r][c] = make_float2(g[0], g[1]);
+            T.guv[r][c] = make_float4(g[2], g[4], g[3], g[5]);
         }
-        T.gl[r][c] = make_float2(g[0], g[1]);
-        T.guv[r][c] = make_float4(g[2], g[4], g[3], g[5]);
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= w || y >= h)
+    const int x = x0 + tx;
+    if (x >= w)
         return;
-    const size_t o = (size_t)y * w + x;
     const bool dense = !J.sparse ||
         (unsigned long long)J.counters[kCntActiveChroma] * 2ull >= (unsigned long long)w * h;
-    if (!dense && J.cmask[o] == 0) {
-        J.ms[o] = 0.0f;
-        return;
-    }
     const bool interior = x0 >= GH && y0 >= GH && x0 + GT_X + GH <= w && y0 + GT_Y + GH <= h;
-    J.ms[o] = interior ? gateAt<true>(T, x, y, x0, y0, w, h) : gateAt<false>(T, x, y, x0, y0, w, h);
+    for (int y = y0 + ty; y < min(y0 + GT_Y, h); y += 8) {
+        const size_t o = (size_t)y * w + x;
+        if (!dense && J.cmask[o] == 0) {
+            J.ms[o] = 0.0f;
+            continue;
+        }
+        J.ms[o] = interior ? gateAt<true>(T, x, y, x0, y0, w, h) : gateAt<false>(T, x, y, x0, y0, w, h);
+    }
 }
 
 } // namespace lgcr_b200

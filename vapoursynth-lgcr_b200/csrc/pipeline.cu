@@ -871,7 +871,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_DIL_V: return J.sparse ? cdiv(J.maskWords, 32) * cdiv(J.sh, 8) : 0;
     case S_MARK: return (J.sparse || J.listed) ? cdiv(J.H * cdiv(J.W, 32), 256) : 0;
     case S_COUNT: return J.sparse ? cdiv(J.cw * J.ch, kCountChunk) : 0;
-    case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, kGateRows) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_HPASS: return (J.hTab && !J.radial && !J.plainFused && (J.kernel != 0 || J.guided)) ? cdiv(J.W, 32) * cdiv(J.ch, 8) : 0;
     case S_PLAIN: return cdiv(J.W, 32) * cdiv(J.H, J.plainRows);
