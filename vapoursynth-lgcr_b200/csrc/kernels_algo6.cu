@@ -133,7 +133,7 @@ k_yc_tiled(LGCR_STAGE_ARGS) {
 }
 
 // 5x5 affine statistics per chroma sample (active samples when sparse).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_affine(LGCR_STAGE_ARGS) {
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -157,21 +157,32 @@ k_affine(LGCR_STAGE_ARGS) {
     for (int k = 0; k < 16; ++k) s[k] = 0.0;
     float mnU = ldf(J.U + (size_t)top * w + left), mxU = mnU;
     float mnV = ldf(J.V + (size_t)top * w + left), mxV = mnV;
-    for (int py = top; py <= bottom; ++py)
-        for (int px = left; px <= right; ++px) {
-            const size_t q = (size_t)py * w + px;
-            const float uf = ldf(J.U + q), vf = ldf(J.V + q);
-            const double u = uf, v = vf;
-            s[0] += u; s[1] += u * u; s[2] += v; s[3] += v * v;
-            mnU = smin(mnU, uf); mxU = smax(mxU, uf);
-            mnV = smin(mnV, vf); mxV = smax(mxV, vf);
+    auto tap = [&](size_t q) {
+        const float uf = ldf(J.U + q), vf = ldf(J.V + q);
+        const double u = uf, v = vf;
+        s[0] += u; s[1] += u * u; s[2] += v; s[3] += v * v;
+        mnU = smin(mnU, uf); mxU = smax(mxU, uf);
+        mnV = smin(mnV, vf); mxV = smax(mxV, vf);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const double ly = ldf(yc[k] + q);
-                const int b = 4 + 4 * k;
-                s[b] += ly; s[b + 1] += ly * ly; s[b + 2] += ly * u; s[b + 3] += ly * v;
-            }
+        for (int k = 0; k < 3; ++k) {
+            const double ly = ldf(yc[k] + q);
+            const int b = 4 + 4 * k;
+            s[b] += ly; s[b + 1] += ly * ly; s[b + 2] += ly * u; s[b + 3] += ly * v;
         }
+    };
+    if (bottom - top == 4 && right - left == 4) {
+        // full 5x5 window: fixed offsets from its first sample
+        const size_t q0 = (size_t)top * w + left;
+#pragma unroll
+        for (int dy = 0; dy < 5; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 5; ++dx)
+                tap(q0 + (size_t)dy * w + dx);
+    } else {
+        for (int py = top; py <= bottom; ++py)
+            for (int px = left; px <= right; ++px)
+                tap((size_t)py * w + px);
+    }
     const int n = (right - left + 1) * (bottom - top + 1);
     const double eps = J.lgfEps;
     const double epsSig = J.epsSig;
