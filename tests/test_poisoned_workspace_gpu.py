@@ -27,6 +27,11 @@ CASES = [
     ("algo4 420P10 jinc3", S.YUV420P10, (64, 48), dict(algo=4, kernel="jinc", taps=3)),
     ("algo6 420P10 lanczos4", S.YUV420P10, (96, 64), dict(algo=6, kernel="lanczos", taps=4)),
     ("algo6 422P10 bilinear", S.YUV422P10, (64, 48), dict(algo=6, kernel="bilinear")),
+    # frames large enough that whole detail-map tiles lie out of every active
+    # pixel's transfer reach and are skipped (30 and 187 tiles here)
+    ("algo6 420P10 720p stretch 2.5", S.YUV420P10, (1280, 720),
+     dict(algo=6, kernel="lanczos", taps=4, stretch=2.5)),
+    ("algo6 420P10 1080p", S.YUV420P10, (1920, 1080), dict(algo=6, kernel="lanczos", taps=4)),
     ("algo6 420PS resize jinc3", S.YUV420PS, (48, 32), dict(algo=6, kernel="jinc", taps=3,
                                                             width=70, height=44)),
     ("bm bp 420P8", S.YUV420P8, (72, 56), dict(algo=2, bm=1, bp=1.0, kernel="lanczos", taps=3)),

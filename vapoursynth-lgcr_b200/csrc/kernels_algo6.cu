@@ -379,6 +379,25 @@ k_detail_map(LGCR_STAGE_ARGS) {
     const int tilesX = (w + kDetailTile - 1) / kDetailTile;
     const int x0 = (tile % tilesX) * kDetailTile, y0 = (tile / tilesX) * rowsOut;
     const int lx = threadIdx.x, tid = threadIdx.y * 32 + lx;
+    if (J.detailReach > 0) {
+        // skip tiles whose samples no active pixel's transfer reads
+        const int reach = J.detailReach;
+        const int xa = max(0, x0 - reach), xb = min(w - 1, x0 + kDetailTile - 1 + reach);
+        const int ya = max(0, y0 - reach), yb = min(h - 1, y0 + rowsOut - 1 + reach);
+        const int wa = xa >> 5, wb = xb >> 5, nw = wb - wa + 1;
+        bool any = false;
+        for (int i = tid; i < (yb - ya + 1) * nw; i += 256) {
+            const int yy = ya + i / nw, wd = wa + i % nw;
+            uint32_t m = __ldg(J.mask + (size_t)yy * J.maskWords + wd);
+            if (wd == wa)
+                m &= ~0u << (xa & 31);
+            if (wd == wb && (xb & 31) != 31)
+                m &= (1u << ((xb & 31) + 1)) - 1u;
+            any |= m != 0;
+        }
+        if (!__syncthreads_or(any))
+            return;
+    }
     const int c = iclamp(x0 - 1 + lx, 0, w - 1);
     const AxisView &ax = J.sax, &ay = J.say;
     const int supY = ay.sup;

@@ -739,6 +739,13 @@ void buildJob(const FrameTask &t, FrameJob &J) {
         J.detailRows = T.detailRows;
         J.detailFused = (J.dTab && !J.radial && J.kernel != 0 && T.sAxSup <= 8 && T.sAySup <= 8 &&
                          T.detailMaxRows <= kDetailStagedRows && J.nyqX <= 1 && J.nyqY <= 1) ? 1 : 0;
+        // The detail transfer reads the map only at active pixels (sparse mask,
+        // same-size output) and bilinearly at +-s along the edge tangent, with
+        // s = 1 + stretch * coherence and coherence <= 1 (the smoothed tensor is
+        // positive semi-definite; 0.1 % margin for rounding): samples more than
+        // floor(1 + stretch) + 2 away from every active pixel are never read.
+        J.detailReach = (J.sparse && J.sameSize)
+            ? int(std::floor(1.0 + double(p.stretch) * 1.001)) + 2 : 0;
     }
     // algo 4
     J.lgf = ws.lgf;

@@ -132,6 +132,8 @@ struct __align__(16) FrameJob {
     int nyqX, nyqY;                    // dyadic Nyquist passes per axis
     int detailFused;                   // k_detail_map builds the detail map in one pass
     int detailRows;                    // output rows per k_detail_map block
+    int detailReach;                   // > 0: detail samples farther than this from every
+                                       // active pixel are never read (tiles skipped)
     int ycTiled;                       // k_yc_tiled builds the degradation candidates
     int sNoClampX, sNoClampY;          // source-grid axes: every chroma tap index in range
     AxisView sax, say;                 // source-grid plain axes (detail map)
