@@ -642,6 +642,22 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     const int tilesX = (w + GT_X - 1) / GT_X;
     const int x0 = (tile % tilesX) * GT_X, y0 = (tile / tilesX) * GT_Y;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool dense = !J.sparse ||
+        (unsigned long long)J.counters[kCntActiveChroma] * 2ull >= (unsigned long long)w * h;
+    if (!dense) {
+        // a tile without active samples only stores the zeros of the gate plane
+        bool any = false;
+        const int x = x0 + tx;
+        if (x < w)
+            for (int y = y0 + ty; y < min(y0 + GT_Y, h); y += 8)
+                any |= J.cmask[(size_t)y * w + x] != 0;
+        if (!__syncthreads_or(any)) {
+            if (x < w)
+                for (int y = y0 + ty; y < min(y0 + GT_Y, h); y += 8)
+                    J.ms[(size_t)y * w + x] = 0.0f;
+            return;
+        }
+    }
     // samples at clamped positions of the tile, its halo and the Sobel ring
     const bool srcInterior = x0 >= GH + 1 && y0 >= GH + 1 && x0 + GT_X + GH + 1 <= w &&
                              y0 + GT_Y + GH + 1 <= h;
@@ -680,8 +696,6 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     const int x = x0 + tx;
     if (x >= w)
         return;
-    const bool dense = !J.sparse ||
-        (unsigned long long)J.counters[kCntActiveChroma] * 2ull >= (unsigned long long)w * h;
     const bool interior = x0 >= GH && y0 >= GH && x0 + GT_X + GH <= w && y0 + GT_Y + GH <= h;
     for (int y = y0 + ty; y < min(y0 + GT_Y, h); y += 8) {
         const size_t o = (size_t)y * w + x;
