@@ -416,12 +416,13 @@ k_dilate_v(LGCR_STAGE_ARGS) {
 }
 
 // ---------------------------------------------------------------------------
-// Sparse workset: one thread per 32 output pixels of a row. An output pixel
-// is active when the mask sample its position maps to is set (every pixel
-// when the frame is not sparse); active pixels mark the 2x2 chroma bilinear
-// footprint. The block counts its active pixels, takes one range of the
-// frame's guided work list with one atomic, and each thread appends its
-// pixels (y << 16 | x) in column order at its prefix offset.
+// Sparse workset: a block covers 256 consecutive 32-pixel words of the
+// output rows; each warp takes 32 of them in turn, one pixel per lane. An
+// output pixel is active when the mask sample its position maps to is set
+// (every pixel when the frame is not sparse); active pixels mark the 2x2
+// chroma bilinear footprint. The block counts its active pixels, takes one
+// range of the frame's guided work list with one atomic, and the lanes
+// append their pixels (y << 16 | x) in raster order at their prefix offsets.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t activeWord(const FrameJob &J, int kw, int oy) {
     const int x0 = kw * 32;
@@ -448,30 +449,17 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
     const int ow = (J.W + 31) / 32;
-    const int idx = tile * 256 + threadIdx.x;
-    const int oy = idx / ow, kw = idx % ow;
-    uint32_t bits = 0;
-    if (oy < J.H) {
-        bits = activeWord(J, kw, oy);
-        if (bits && J.sparse) {
-            const int cy0 = __ldg(J.ay.cbI0 + oy);
-            const int cy1 = min(cy0 + 1, J.ch - 1);
-            uint8_t *row0 = J.cmask + (size_t)cy0 * J.cw;
-            uint8_t *row1 = J.cmask + (size_t)cy1 * J.cw;
-            int written = -1;
-            for (uint32_t m = bits; m; m &= m - 1) {
-                const int ox = kw * 32 + __ffs(m) - 1;
-                const int cx0 = __ldg(J.ax.cbI0 + ox);
-                const int cx1 = min(cx0 + 1, J.cw - 1);
-                if (cx0 > written) { row0[cx0] = 1; row1[cx0] = 1; }
-                if (cx1 > written) { row0[cx1] = 1; row1[cx1] = 1; }
-                written = max(written, cx1);
-            }
-        }
-    }
-    // block prefix of the active counts
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned cnt = __popc(bits);
+    const int wordBase = tile * 256 + warp * 32;          // this warp's 32 words
+    // pass 1: lane i counts word wordBase + i
+    uint32_t myBits = 0;
+    {
+        const int idx = wordBase + lane;
+        const int oy = idx / ow, kw = idx - oy * ow;
+        if (oy < J.H)
+            myBits = activeWord(J, kw, oy);
+    }
+    const unsigned cnt = __popc(myBits);
     unsigned incl = cnt;
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned n = __shfl_up_sync(0xffffffffu, incl, o);
@@ -490,11 +478,32 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
         blockBase = total ? atomicAdd(J.counters + kCntActiveOutput, (unsigned long long)total) : 0ull;
     }
     __syncthreads();
-    if (bits && J.listed) {
-        unsigned long long pos = blockBase + warpCount[warp] + incl - cnt;
-        const uint32_t rowCode = (uint32_t)oy << 16;
-        for (uint32_t m = bits; m; m &= m - 1)
-            J.actList[pos++] = rowCode | (uint32_t)(kw * 32 + __ffs(m) - 1);
+    const unsigned long long warpBase = blockBase + warpCount[warp];
+    const unsigned excl = incl - cnt;
+    const uint32_t below = (1u << lane) - 1u;
+    // pass 2: the warp walks its words, one pixel per lane
+    for (int i = 0; i < 32; ++i) {
+        const uint32_t bits = __shfl_sync(0xffffffffu, myBits, i);
+        const unsigned offs = __shfl_sync(0xffffffffu, excl, i);
+        if (!bits)
+            continue;                                      // warp-uniform
+        if (!((bits >> lane) & 1u))
+            continue;
+        const int idx = wordBase + i;
+        const int oy = idx / ow, kw = idx - oy * ow;
+        const int ox = kw * 32 + lane;
+        if (J.sparse) {
+            const int cy0 = __ldg(J.ay.cbI0 + oy);
+            const int cy1 = min(cy0 + 1, J.ch - 1);
+            const int cx0 = __ldg(J.ax.cbI0 + ox);
+            const int cx1 = min(cx0 + 1, J.cw - 1);
+            uint8_t *row0 = J.cmask + (size_t)cy0 * J.cw;
+            uint8_t *row1 = J.cmask + (size_t)cy1 * J.cw;
+            row0[cx0] = 1; row0[cx1] = 1;
+            row1[cx0] = 1; row1[cx1] = 1;
+        }
+        if (J.listed)
+            J.actList[warpBase + offs + __popc(bits & below)] = ((uint32_t)oy << 16) | (uint32_t)ox;
     }
 }
 
