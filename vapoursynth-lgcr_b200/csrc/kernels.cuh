@@ -21,14 +21,17 @@ constexpr size_t kPlainDynSmem = size_t(kPlainStagedRows) * 32 * (8 + 16 + 8);
 // k_detail_map: most horizontal-table rows one block stages.
 constexpr int kDetailStagedRows = 40;
 
-// k_convert: samples per warp (one row segment) and warps per block; the
-// luma blocks of a frame come first, then the chroma blocks.
+// k_convert: samples per warp (one row segment: luma, chroma) and warps per
+// block; the luma blocks of a frame come first, then the chroma blocks.
+constexpr int kConvertLumaSpan = 512;
 constexpr int kConvertSpan = 256;
 constexpr int kConvertWarps = 8;
-__host__ __device__ __forceinline__ int convertBlocks(int w, int h) {
-    return (h * ((w + kConvertSpan - 1) / kConvertSpan) + kConvertWarps - 1) / kConvertWarps;
+__host__ __device__ __forceinline__ int convertBlocks(int w, int h, int span = kConvertSpan) {
+    return (h * ((w + span - 1) / span) + kConvertWarps - 1) / kConvertWarps;
 }
-__host__ __device__ __forceinline__ int convertLumaBlocks(int sw, int sh) { return convertBlocks(sw, sh); }
+__host__ __device__ __forceinline__ int convertLumaBlocks(int sw, int sh) {
+    return convertBlocks(sw, sh, kConvertLumaSpan);
+}
 
 // k_tensor: columns each warp emits, warps per block (side by side), rows
 // per strip.

@@ -16,8 +16,9 @@ namespace lgcr_b200 {
 
 // ---------------------------------------------------------------------------
 // Input conversion with the footprint luma map folded in. A warp converts
-// kConvertSpan consecutive samples of one row, lane l taking samples l,
-// l + 32, ... so every load and store is one coalesced row segment. The
+// one row segment (kConvertLumaSpan luma samples, 8 consecutive per lane and
+// both halves' loads in flight together; kConvertSpan chroma samples, lane l
+// taking samples l, l + 32, ...), so every load and store is coalesced. The
 // first convertLumaBlocks(J) blocks of a frame cover the luma plane (and copy
 // it to a same-size output), the rest the chroma planes; the chroma blocks
 // also clear the chroma work masks and compute lc from the luma codes.
@@ -94,8 +95,9 @@ __device__ __forceinline__ void rawStore8(char *row, int x, const uint32_t (&raw
         rawStore<KIND>(row, x + k, raw[k]);
 }
 
-// Luma: each lane converts 8 consecutive samples (one vector load) of the
-// warp's 256-sample row segment; unaligned rows take the per-sample path.
+// Luma: each lane converts 8 consecutive samples (one vector load) in each
+// half of the warp's row segment, both loads issued before any store;
+// unaligned rows take the per-sample path.
 template <int KIND>
 __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, int lane) {
     const char *src = static_cast<const char *>(J.in[0]) + (long long)y * J.inPitch[0];
@@ -104,79 +106,128 @@ __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, in
     float *yw = J.Yw ? J.Yw + (size_t)y * J.sw : nullptr;
     const double scale = J.yScale;
     const int w = J.sw;
-    const int x = xb + lane * 8;
-    if (x >= w)
-        return;
-    uint32_t raw[8];
-    if (x + 8 <= w && rawLoad8<KIND>(src, x, raw)) {
-        if (yw) {
-            float v[8];
+    constexpr int half = kConvertLumaSpan / 2;
+    uint32_t raw[2][8];
+    bool vec[2];
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                v[k] = rawToFloat<KIND>(raw[k], scale, 0.0);
-            if (!(reinterpret_cast<uintptr_t>(yw + x) & 15)) {
-                reinterpret_cast<float4 *>(yw + x)[0] = make_float4(v[0], v[1], v[2], v[3]);
-                reinterpret_cast<float4 *>(yw + x)[1] = make_float4(v[4], v[5], v[6], v[7]);
-            } else {
+    for (int s = 0; s < 2; ++s) {
+        const int x = xb + s * half + lane * 8;
+        vec[s] = x + 8 <= w && rawLoad8<KIND>(src, x, raw[s]);
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int x = xb + s * half + lane * 8;
+        if (x >= w)
+            continue;
+        if (vec[s]) {
+            if (yw) {
+                float v[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
-                    yw[x + k] = v[k];
+                    v[k] = rawToFloat<KIND>(raw[s][k], scale, 0.0);
+                if (!(reinterpret_cast<uintptr_t>(yw + x) & 15)) {
+                    reinterpret_cast<float4 *>(yw + x)[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    reinterpret_cast<float4 *>(yw + x)[1] = make_float4(v[4], v[5], v[6], v[7]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        yw[x + k] = v[k];
+                }
             }
+            if (dst)
+                rawStore8<KIND>(dst, x, raw[s]);
+            continue;
         }
-        if (dst)
-            rawStore8<KIND>(dst, x, raw);
-        return;
-    }
-    for (int k = 0; k < 8 && x + k < w; ++k) {
-        const uint32_t r = rawLoad<KIND>(src, x + k);
-        if (yw)
-            yw[x + k] = rawToFloat<KIND>(r, scale, 0.0);
-        if (dst)
-            rawStore<KIND>(dst, x + k, r);
+        for (int k = 0; k < 8 && x + k < w; ++k) {
+            const uint32_t r = rawLoad<KIND>(src, x + k);
+            if (yw)
+                yw[x + k] = rawToFloat<KIND>(r, scale, 0.0);
+            if (dst)
+                rawStore<KIND>(dst, x + k, r);
+        }
     }
 }
 
+// Chroma: groups of two samples per lane; a group's loads (U, V and, for
+// the usual 2x2 footprint, the four luma codes of lc) are issued before its
+// stores, which go through restrict-qualified pointers.
 template <int KIND>
 __device__ __forceinline__ void convertChroma(const FrameJob &J, int cy, int xb, int lane) {
     const char *su = static_cast<const char *>(J.in[1]) + (long long)cy * J.inPitch[1];
     const char *sv = static_cast<const char *>(J.in[2]) + (long long)cy * J.inPitch[2];
     const size_t rowOff = (size_t)cy * J.cw;
     const double scale = J.yScale, off = J.cOffset;
+    float *__restrict__ uw = J.Uw;
+    float *__restrict__ vw = J.Vw;
+    double2 *__restrict__ uvd = reinterpret_cast<double2 *>(J.uvd);
+    uint8_t *__restrict__ cmask = J.cmask;
+    uint8_t *__restrict__ roi = J.roi;
+    float *__restrict__ lc = J.lc;
     int yb = 0, ye = 0;
     const char *lrow0 = nullptr;
     const long long lpitch = J.inPitch[0];
-    if (J.lc) {
+    if (lc) {
         yb = __ldg(J.lcYb + cy);
         ye = __ldg(J.lcYe + cy);
         lrow0 = static_cast<const char *>(J.in[0]) + (long long)yb * lpitch;
     }
-#pragma unroll 2
-    for (int k = 0; k < kConvertSpan / 32; ++k) {
-        const int cx = xb + lane + 32 * k;
-        if (cx >= J.cw)
-            break;
-        const size_t o = rowOff + cx;
-        const float u = rawToFloat<KIND>(rawLoad<KIND>(su, cx), scale, off);
-        const float v = rawToFloat<KIND>(rawLoad<KIND>(sv, cx), scale, off);
-        if (J.Uw) J.Uw[o] = u;
-        if (J.Vw) J.Vw[o] = v;
-        if (J.uvd) reinterpret_cast<double2 *>(J.uvd)[o] = make_double2((double)u, (double)v);
-        if (J.cmask) J.cmask[o] = 0;
-        if (J.roi) J.roi[o] = 0;
-        if (J.lc) {
-            // buildLcMap: raster-order double sum over the footprint
-            const int xb0 = __ldg(J.lcXb + cx), xe0 = __ldg(J.lcXe + cx);
-            double sum = 0.0;
-            const char *lrow = lrow0;
-            for (int j = yb; j < ye; ++j, lrow += lpitch)
-                for (int i = xb0; i < xe0; ++i)
-                    sum += (double)rawToFloat<KIND>(rawLoad<KIND>(lrow, i), scale, 0.0);
-            J.lc[o] = (float)(sum / ((double)(xe0 - xb0) * (double)(ye - yb)));
+    constexpr int kGroup = 2;
+#pragma unroll 1
+    for (int g = 0; g < kConvertSpan / 32; g += kGroup) {
+        uint32_t ru[kGroup], rv[kGroup], fp[kGroup][4];
+        int fxb[kGroup], fxe[kGroup];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int cx = xb + lane + 32 * (g + k);
+            if (cx >= J.cw)
+                break;
+            ru[k] = rawLoad<KIND>(su, cx);
+            rv[k] = rawLoad<KIND>(sv, cx);
+            if (lc) {
+                fxb[k] = __ldg(J.lcXb + cx);
+                fxe[k] = __ldg(J.lcXe + cx);
+                if (fxe[k] - fxb[k] == 2 && ye - yb == 2) {
+                    fp[k][0] = rawLoad<KIND>(lrow0, fxb[k]);
+                    fp[k][1] = rawLoad<KIND>(lrow0, fxb[k] + 1);
+                    fp[k][2] = rawLoad<KIND>(lrow0 + lpitch, fxb[k]);
+                    fp[k][3] = rawLoad<KIND>(lrow0 + lpitch, fxb[k] + 1);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int cx = xb + lane + 32 * (g + k);
+            if (cx >= J.cw)
+                break;
+            const size_t o = rowOff + cx;
+            const float u = rawToFloat<KIND>(ru[k], scale, off);
+            const float v = rawToFloat<KIND>(rv[k], scale, off);
+            if (uw) uw[o] = u;
+            if (vw) vw[o] = v;
+            if (uvd) uvd[o] = make_double2((double)u, (double)v);
+            if (cmask) cmask[o] = 0;
+            if (roi) roi[o] = 0;
+            if (lc) {
+                // buildLcMap: raster-order double sum over the footprint
+                const int xb0 = fxb[k], xe0 = fxe[k];
+                double sum = 0.0;
+                if (xe0 - xb0 == 2 && ye - yb == 2) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        sum += (double)rawToFloat<KIND>(fp[k][q], scale, 0.0);
+                } else {
+                    const char *lrow = lrow0;
+                    for (int j = yb; j < ye; ++j, lrow += lpitch)
+                        for (int i = xb0; i < xe0; ++i)
+                            sum += (double)rawToFloat<KIND>(rawLoad<KIND>(lrow, i), scale, 0.0);
+                }
+                lc[o] = (float)(sum / ((double)(xe0 - xb0) * (double)(ye - yb)));
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(kConvertWarps * 32)
+__global__ void __launch_bounds__(kConvertWarps * 32, 3)
 k_convert(LGCR_STAGE_ARGS) {
     __shared__ FrameJob sJob;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
@@ -186,13 +237,13 @@ k_convert(LGCR_STAGE_ARGS) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lumaBlocks = convertLumaBlocks(J.sw, J.sh);
     if (tile < lumaBlocks) {
-        const int gpr = (J.sw + kConvertSpan - 1) / kConvertSpan;
+        const int gpr = (J.sw + kConvertLumaSpan - 1) / kConvertLumaSpan;
         const int gw = tile * kConvertWarps + warp;
         if (gw >= J.sh * gpr)
             return;
         if (gw == 0 && lane < kCntCount)
             J.counters[lane] = 0ull;
-        const int y = gw / gpr, xb = (gw % gpr) * kConvertSpan;
+        const int y = gw / gpr, xb = (gw % gpr) * kConvertLumaSpan;
         switch (J.inKind) {
         case kU8: convertLuma<kU8>(J, y, xb, lane); break;
         case kU16: convertLuma<kU16>(J, y, xb, lane); break;

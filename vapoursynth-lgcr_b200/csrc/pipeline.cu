@@ -869,7 +869,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
         return (J.guided && J.algo == 6 && !J.detailFused && pass < J.nyqX + J.nyqY) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
     }
     switch (s) {
-    case S_CONVERT: return convertBlocks(J.sw, J.sh) + convertBlocks(J.cw, J.ch);
+    case S_CONVERT: return convertLumaBlocks(J.sw, J.sh) + convertBlocks(J.cw, J.ch);
     case S_LUMA_RADIAL: return (resize && J.writeLuma && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_LUMA_H: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_LUMA_V: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
