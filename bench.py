@@ -126,12 +126,14 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def read_traffic():
-    """Per-launch DRAM traffic of the dominant stage from the committed ncu
-    summary (line 'traffic_bytes_per_output_pixel: X'), scaled by pixels."""
+def read_traffic(stage):
+    """DRAM traffic per output pixel of one stage's kernel from the committed
+    ncu summary (line 'traffic_bytes_per_output_pixel <stage>: X'); the
+    caller scales it by the pixels of one launch. None when not captured."""
     path = os.path.join(ROOT, "profiles", "recon_kernels_batched_8frames.md")
     try:
-        m = re.search(r"traffic_bytes_per_output_pixel:\s*([0-9.eE+-]+)", open(path).read())
+        m = re.search(r"traffic_bytes_per_output_pixel %s:\s*([0-9.eE+-]+)" % re.escape(stage),
+                      open(path).read())
         return float(m.group(1)) if m else None
     except Exception:
         return None
@@ -569,7 +571,7 @@ def our_arm(args):
         algo_bytes = BYTES_PER_PIXEL * out_pixels
         achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
-        tpp = read_traffic()
+        tpp = read_traffic(dominant)
         rl = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
               "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
               "traffic": (round(tpp * out_pixels) if tpp else None),
