@@ -581,13 +581,9 @@ __device__ __forceinline__ bool activeOut(const FrameJob &J, int ox, int oy) {
     return maskAt(J, mx, my) != 0;
 }
 
-__global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    const FrameJob &J = jobs[f];
-    int ox, oy;
-    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
-    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
-        return;
+// Detail transfer of one active output pixel (detailTransferImpl,
+// src/algos.cpp:1587-1698).
+__device__ __forceinline__ void transferPixel(const FrameJob &J, int ox, int oy) {
     const AxisView &ax = J.ax, &ay = J.ay;
     const int lxi = __ldg(ax.lbI0 + ox), lyi = __ldg(ay.lbI0 + oy);
     const float lxf = __ldg(ax.lbF + ox), lyf = __ldg(ay.lbF + oy);
@@ -641,6 +637,54 @@ __global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
     } else {
         J.oU[o] = ou;
         J.oV[o] = ov;
+    }
+}
+__global__ void k_detail_transfer(LGCR_STAGE_ARGS) {
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    const FrameJob &J = jobs[f];
+    int ox, oy;
+    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
+    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
+        return;
+    transferPixel(J, ox, oy);
+}
+
+// Sparse frames: a persistent grid walks the frames' compacted work lists of
+// active output pixels (built by the workset stage), so no lane idles on an
+// inactive pixel. Each block builds the prefix of the listed frames' list
+// lengths in shared memory and strides over the concatenated work.
+constexpr int kXferMaxFrames = 1024;
+
+__global__ void __launch_bounds__(256)
+k_detail_transfer_list(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    __shared__ unsigned long long pre[kXferMaxFrames + 1];
+    for (int chunk = 0; chunk < njobs; chunk += kXferMaxFrames) {
+        const int n = min(kXferMaxFrames, njobs - chunk);
+        if (threadIdx.x == 0) {
+            unsigned long long acc = 0;
+            for (int i = 0; i < n; ++i) {
+                pre[i] = acc;
+                const FrameJob &J = jobs[chunk + i];
+                if (J.xferListed)
+                    acc += J.counters[kCntActiveOutput];
+            }
+            pre[n] = acc;
+        }
+        __syncthreads();
+        const unsigned long long total = pre[n];
+        for (unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+             w += (unsigned long long)gridDim.x * blockDim.x) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pre[mid] <= w) lo = mid; else hi = mid - 1;
+            }
+            const FrameJob &J = jobs[chunk + lo];
+            const uint32_t pix = __ldg(J.actList + (w - pre[lo]));
+            transferPixel(J, (int)(pix & 0xffffu), (int)(pix >> 16));
+        }
+        __syncthreads();
     }
 }
 

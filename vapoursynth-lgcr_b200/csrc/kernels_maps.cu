@@ -553,7 +553,7 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
             row0[cx0] = 1; row0[cx1] = 1;
             row1[cx0] = 1; row1[cx1] = 1;
         }
-        if (J.listed)
+        if (J.listed || J.xferListed)
             J.actList[warpBase + offs + __popc(bits & below)] = ((uint32_t)oy << 16) | (uint32_t)ox;
     }
 }

@@ -490,7 +490,7 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     const bool listed = guided && (p.algo == 2 || p.algo == 4);
     Slot sUvd = take(C * 16), sHTab = take(size_t(p.outW) * ch * 32, !p.k.radial);
     Slot sWExt = take(O * 24, listed && !p.k.radial && p.k.kernel != Kernel::Bilinear);
-    Slot sList = take(O * 4, listed);
+    Slot sList = take(O * 4, listed || (guided && p.algo == 6 && p.sparse));
     const bool algo6 = guided && p.algo == 6, algo4 = guided && p.algo == 4;
     Slot sAff = take(9 * C * 4, algo6), sYc1 = take(C * 4, algo6), sYc2 = take(C * 4, algo6);
     Slot sDt1 = take(L * 4, algo6), sDt2 = take(L * 4, algo6);
@@ -689,6 +689,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.hTab = ws.hTab;
     J.actList = ws.actList;
     J.listed = J.guided && (p.algo == 2 || p.algo == 4);
+    J.xferListed = (J.guided && p.algo == 6 && J.sparse && ws.actList) ? 1 : 0;
     {
         // guided bump denominator 1 + dp^2/g^2 + dt^2/(g*aniso)^2 with aniso >= 1:
         // |dp|, |dt| <= (tap distance in chroma samples) * ratio * |n| summed
@@ -772,7 +773,7 @@ enum StageId : int {
     S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_DIL_H, S_DIL_V,
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
     S_YC, S_YC_TILED, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
-    S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER,
+    S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER, S_DET_XFER_LIST,
     S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
 
@@ -789,7 +790,7 @@ const char *stageName(int s) {
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
         "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
         "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
-        "selector_roi", "buildLGF_roi", "selectorBlend", "collaborative_chroma_group",
+        "detailTransfer_listed", "selector_roi", "buildLGF_roi", "selectorBlend", "collaborative_chroma_group",
         "collaborative_chroma", "backProject", "output_conversion",
     };
     return (s >= 0 && s < S_N) ? names[s] : "unknown";
@@ -892,7 +893,8 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_DET_RH: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_RV: return (J.guided && J.algo == 6 && resize && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_DET_RR: return (J.guided && J.algo == 6 && resize && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
-    case S_DET_TRANSFER: return (J.guided && J.algo == 6) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_DET_TRANSFER: return (J.guided && J.algo == 6 && !J.xferListed) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_DET_XFER_LIST: return J.xferListed ? 1 : 0;
     case S_ROI:
     case S_BLEND: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_BM_GROUP: return J.bm ? cdiv(J.bmAnchorsX * J.bmAnchorsY, 8) : 0;
@@ -999,6 +1001,19 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_DET_RV, k_detail_resize_v, b32x8);
     go(S_DET_RR, k_detail_resize_radial, b32x8);
     go(S_DET_TRANSFER, k_detail_transfer, b32x8);
+    if (plan.totals[S_DET_XFER_LIST] > 0) {
+        // persistent grid over the algo 6 frames' work lists
+        static int gridBlocks = 0;
+        if (gridBlocks == 0) {
+            int dev = 0, sms = 0, perSm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_detail_transfer_list, 256, 0);
+            gridBlocks = std::max(1, sms * std::max(1, perSm));
+        }
+        k_detail_transfer_list<<<gridBlocks, 256, 0, stream>>>(dJobs, pre(S_DET_XFER_LIST), n);
+        ++launches;
+    }
     go(S_ROI, k_roi, b32x8);
     go(S_LGF_ROI, k_lgf, b32x8);
     go(S_BLEND, k_blend, b32x8);

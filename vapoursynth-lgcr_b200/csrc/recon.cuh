@@ -115,6 +115,7 @@ struct __align__(16) FrameJob {
     double *uvd;                       // cw x ch x 2: (u, v) in FP64
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
+    int xferListed;                    // algo 6: detail transfer walks the work list
     int bumpRcpSafe;                   // every guided bump denominator stays below 2^64
     int plainFused;                    // k_plain computes its horizontal rows itself
     int plainRows;                     // output rows per k_plain block
