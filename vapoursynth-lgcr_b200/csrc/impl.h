@@ -97,6 +97,7 @@ struct Workspace {
     float *hTab = nullptr;
     float *wExt = nullptr;              // W x H float4 hull plane, then W x H float2 luma plane
     uint32_t *actList = nullptr;
+    uint32_t *chromaList = nullptr;
     float *aff = nullptr, *yc1 = nullptr, *yc2 = nullptr, *ycTmp = nullptr;
     float *detail = nullptr, *detailTmp = nullptr, *detailTmp2 = nullptr, *dTab = nullptr;
     float *lgf = nullptr, *selW2 = nullptr, *selW3 = nullptr, *gU = nullptr, *gV = nullptr;

@@ -87,6 +87,7 @@ __global__ void k_detail_resize_v(LGCR_STAGE_ARGS);
 __global__ void k_detail_resize_radial(LGCR_STAGE_ARGS);
 __global__ void k_detail_transfer(LGCR_STAGE_ARGS);
 __global__ void k_detail_transfer_list(LGCR_STAGE_ARGS);
+__global__ void k_affine_list(LGCR_STAGE_ARGS);
 // algo 4
 __global__ void k_lgf(LGCR_STAGE_ARGS);
 __global__ void k_roi(LGCR_STAGE_ARGS);

@@ -132,23 +132,16 @@ k_yc_tiled(LGCR_STAGE_ARGS) {
     }
 }
 
-// 5x5 affine statistics per chroma sample (active samples when sparse).
-__global__ void __launch_bounds__(256, 3)
-k_affine(LGCR_STAGE_ARGS) {
-    __shared__ FrameJob sJob;
-    const int f = findFrame(tileStart, njobs, blockIdx.x);
-    stageJob(jobs, f, sJob);
-    const FrameJob &J = sJob;
-    int x, y;
-    tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
+// 5x5 affine statistics of one chroma sample (buildAffineMaps,
+// src/algos.cpp:1026-1526).
+__device__ __forceinline__ bool affineSparse(const FrameJob &J) {
+    return J.sparse && (unsigned long long)J.counters[kCntActiveChroma] * 2ull <
+                           (unsigned long long)J.cw * J.ch;
+}
+
+__device__ __forceinline__ void affineSample(const FrameJob &J, int x, int y, bool sparseRoi) {
     const int w = J.cw, h = J.ch;
-    if (x >= w || y >= h)
-        return;
     const size_t o = (size_t)y * w + x;
-    const bool sparseRoi = J.sparse &&
-        (unsigned long long)J.counters[kCntActiveChroma] * 2ull < (unsigned long long)w * h;
-    if (sparseRoi && J.cmask[o] == 0)
-        return;
     const int top = max(0, y - 2), bottom = min(h - 1, y + 2);
     const int left = max(0, x - 2), right = min(w - 1, x + 2);
     const float *yc[3] = { J.lc, J.yc1, J.yc2 };
@@ -214,6 +207,72 @@ k_affine(LGCR_STAGE_ARGS) {
     // interleaved maps: (aU, aV, g, rng) then (mnU, mxU, mnV, mxV) per sample
     reinterpret_cast<float4 *>(J.aff)[o] = make_float4(slopeU, slopeV, gain, smax(mxU - mnU, mxV - mnV));
     reinterpret_cast<float4 *>(J.aff + 4 * C)[o] = make_float4(mnU, mxU, mnV, mxV);
+}
+
+// Tiled form (frames without a chroma work list): active samples when sparse.
+__global__ void __launch_bounds__(256, 3)
+k_affine(LGCR_STAGE_ARGS) {
+    __shared__ FrameJob sJob;
+    const int f = findFrame(tileStart, njobs, blockIdx.x);
+    stageJob(jobs, f, sJob);
+    const FrameJob &J = sJob;
+    int x, y;
+    tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
+    if (x >= J.cw || y >= J.ch)
+        return;
+    const bool sparseRoi = affineSparse(J);
+    if (sparseRoi && J.cmask[(size_t)y * J.cw + x] == 0)
+        return;
+    affineSample(J, x, y, sparseRoi);
+}
+
+// Sparse frames: a persistent grid walks the compacted list of active chroma
+// samples (every sample, in raster order, once the frame counts as dense),
+// so no lane idles on an inactive sample.
+constexpr int kAffineMaxFrames = 1024;
+
+__global__ void __launch_bounds__(256, 3)
+k_affine_list(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    __shared__ unsigned long long pre[kAffineMaxFrames + 1];
+    for (int chunk = 0; chunk < njobs; chunk += kAffineMaxFrames) {
+        const int n = min(kAffineMaxFrames, njobs - chunk);
+        if (threadIdx.x == 0) {
+            unsigned long long acc = 0;
+            for (int i = 0; i < n; ++i) {
+                pre[i] = acc;
+                const FrameJob &J = jobs[chunk + i];
+                if (J.chromaList)
+                    acc += affineSparse(J) ? J.counters[kCntActiveChroma]
+                                           : (unsigned long long)J.cw * J.ch;
+            }
+            pre[n] = acc;
+        }
+        __syncthreads();
+        const unsigned long long total = pre[n];
+        for (unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+             w += (unsigned long long)gridDim.x * blockDim.x) {
+            int lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pre[mid] <= w) lo = mid; else hi = mid - 1;
+            }
+            const FrameJob &J = jobs[chunk + lo];
+            const unsigned long long k = w - pre[lo];
+            const bool sparseRoi = affineSparse(J);
+            int x, y;
+            if (sparseRoi) {
+                const uint32_t e = __ldg(J.chromaList + k);
+                x = (int)(e & 0xffffu);
+                y = (int)(e >> 16);
+            } else {
+                y = (int)(k / (unsigned long long)J.cw);
+                x = (int)(k - (unsigned long long)y * J.cw);
+            }
+            affineSample(J, x, y, sparseRoi);
+        }
+        __syncthreads();
+    }
 }
 
 // Horizontal pass of the degraded-luma reconstruction (separable kernels):

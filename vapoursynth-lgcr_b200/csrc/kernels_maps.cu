@@ -558,38 +558,62 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
     }
 }
 
-// Active chroma samples: population count of the 0/1 chroma mask bytes,
-// 16 bytes per thread per step, one atomic per block.
+// Active chroma samples: population count of the 0/1 chroma mask bytes, a
+// contiguous 64-byte span per thread, one atomic per block. Frames with a
+// chroma work list also get their active samples (y << 16 | x) appended in
+// raster order at the block's range.
 __global__ void __launch_bounds__(256)
 k_count(LGCR_STAGE_ARGS) {
     __shared__ unsigned warpSum[8];
+    __shared__ unsigned long long blockBase;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
     const size_t nc = (size_t)J.cw * J.ch;
-    const size_t base = (size_t)tile * kCountChunk;
-    const size_t end = min(nc, base + kCountChunk);
+    const size_t span = (size_t)tile * kCountChunk + (size_t)threadIdx.x * (kCountChunk / 256);
+    const size_t spanEnd = min(nc, span + kCountChunk / 256);
     unsigned c = 0;
-    for (size_t i = base + threadIdx.x * 16; i < end; i += 256 * 16) {
-        if (i + 16 <= end) {
-            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(J.cmask + i));
+    if (span + kCountChunk / 256 <= nc) {
+#pragma unroll
+        for (int k = 0; k < kCountChunk / 256 / 16; ++k) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(J.cmask + span) + k);
             c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
-        } else {
-            for (size_t k = i; k < end; ++k)
-                c += J.cmask[k] != 0;
         }
+    } else {
+        for (size_t k = span; k < spanEnd; ++k)
+            c += J.cmask[k] != 0;
     }
-    for (int o = 16; o > 0; o >>= 1)
-        c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0)
-        warpSum[threadIdx.x >> 5] = c;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned n = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += n;
+    }
+    if (lane == 31)
+        warpSum[warp] = incl;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned total = 0;
-        for (int i = 0; i < 8; ++i)
-            total += warpSum[i];
-        if (total)
-            atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)total);
+        for (int i = 0; i < 8; ++i) {
+            const unsigned w = warpSum[i];
+            warpSum[i] = total;
+            total += w;
+        }
+        blockBase = total ? atomicAdd(J.counters + kCntActiveChroma, (unsigned long long)total) : 0ull;
+    }
+    __syncthreads();
+    if (J.chromaList && c) {
+        unsigned long long pos = blockBase + warpSum[warp] + incl - c;
+        int y = (int)(span / (size_t)J.cw);
+        int x = (int)(span - (size_t)y * J.cw);
+        for (size_t k = span; k < spanEnd; ++k) {
+            if (J.cmask[k])
+                J.chromaList[pos++] = ((uint32_t)y << 16) | (uint32_t)x;
+            if (++x == J.cw) {
+                x = 0;
+                ++y;
+            }
+        }
     }
 }
 

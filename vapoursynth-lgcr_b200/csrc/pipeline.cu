@@ -491,6 +491,7 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     Slot sUvd = take(C * 16), sHTab = take(size_t(p.outW) * ch * 32, !p.k.radial);
     Slot sWExt = take(O * 24, listed && !p.k.radial && p.k.kernel != Kernel::Bilinear);
     Slot sList = take(O * 4, listed || (guided && p.algo == 6 && p.sparse));
+    Slot sCList = take(C * 4, guided && p.algo == 6 && p.sparse);
     const bool algo6 = guided && p.algo == 6, algo4 = guided && p.algo == 4;
     Slot sAff = take(9 * C * 4, algo6), sYc1 = take(C * 4, algo6), sYc2 = take(C * 4, algo6);
     Slot sDt1 = take(L * 4, algo6), sDt2 = take(L * 4, algo6);
@@ -530,6 +531,7 @@ std::unique_ptr<Workspace> Filter::makeWorkspace(bool hostStaging) {
     ws->hTab = F(sHTab);
     ws->wExt = F(sWExt);
     ws->actList = sList.on ? (uint32_t *)ar.at(sList.off) : nullptr;
+    ws->chromaList = sCList.on ? (uint32_t *)ar.at(sCList.off) : nullptr;
     ws->aff = F(sAff); ws->yc1 = F(sYc1); ws->yc2 = F(sYc2);
     ws->detailTmp = F(sDt1); ws->detailTmp2 = F(sDt2); ws->detail = F(sDet); ws->dTab = F(sDTab);
     (void)sLumaTmp2;
@@ -690,6 +692,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.actList = ws.actList;
     J.listed = J.guided && (p.algo == 2 || p.algo == 4);
     J.xferListed = (J.guided && p.algo == 6 && J.sparse && ws.actList) ? 1 : 0;
+    J.chromaList = (J.guided && p.algo == 6 && J.sparse) ? ws.chromaList : nullptr;
     {
         // guided bump denominator 1 + dp^2/g^2 + dt^2/(g*aniso)^2 with aniso >= 1:
         // |dp|, |dt| <= (tap distance in chroma samples) * ratio * |n| summed
@@ -772,7 +775,7 @@ void buildJob(const FrameTask &t, FrameJob &J) {
 enum StageId : int {
     S_CONVERT, S_LUMA_RADIAL, S_LUMA_H, S_LUMA_V, S_TENSOR, S_DIL_H, S_DIL_V,
     S_MARK, S_COUNT, S_GATE, S_LGF_DENSE, S_HPASS, S_PLAIN, S_GUIDED,
-    S_YC, S_YC_TILED, S_AFFINE, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
+    S_YC, S_YC_TILED, S_AFFINE, S_AFFINE_LIST, S_DET_HPASS, S_DET_PLAIN, S_DET_MAP, S_NYQ0, S_NYQ1, S_NYQ2, S_NYQ3, S_NYQ4, S_NYQ5, S_NYQ6, S_NYQ7,
     S_DET_RH, S_DET_RV, S_DET_RR, S_DET_TRANSFER, S_DET_XFER_LIST,
     S_ROI, S_LGF_ROI, S_BLEND, S_BM_GROUP, S_BM_AGG, S_BP, S_STORE, S_N
 };
@@ -786,7 +789,7 @@ const char *stageName(int s) {
         "input_conversion", "luma_resample_radial", "luma_resample_h", "luma_resample_v",
         "buildGuideMaps_tensor", "buildTrustMask_h", "buildTrustMask_v",
         "buildSparseWorkset", "buildSparseWorkset_count", "buildMutualGate", "buildLGF",
-        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps_candidates_tiled", "buildAffineMaps", "buildDetail_horizontal", "buildDetail_plain", "buildDetailMap",
+        "plainChroma_horizontal", "plainChroma", "reconstructChroma", "buildAffineMaps_candidates", "buildAffineMaps_candidates_tiled", "buildAffineMaps", "buildAffineMaps_listed", "buildDetail_horizontal", "buildDetail_plain", "buildDetailMap",
         "buildDetail_nyquist0", "buildDetail_nyquist1", "buildDetail_nyquist2", "buildDetail_nyquist3",
         "buildDetail_nyquist4", "buildDetail_nyquist5", "buildDetail_nyquist6", "buildDetail_nyquist7",
         "buildDetail_resize_h", "buildDetail_resize_v", "buildDetail_resize_radial", "detailTransfer",
@@ -886,7 +889,8 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_GUIDED: return J.listed ? 1 : 0;
     case S_YC: return (J.guided && J.algo == 6 && !J.ycTiled) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_YC_TILED: return (J.guided && J.algo == 6 && J.ycTiled) ? cdiv(J.cw, kYcTile) * cdiv(J.ch, kYcTile) : 0;
-    case S_AFFINE: return (J.guided && J.algo == 6) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_AFFINE: return (J.guided && J.algo == 6 && !J.chromaList) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
+    case S_AFFINE_LIST: return J.chromaList ? 1 : 0;
     case S_DET_HPASS: return (J.guided && J.algo == 6 && J.dTab && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.ch, 8) : 0;
     case S_DET_PLAIN: return (J.guided && J.algo == 6 && !J.detailFused) ? cdiv(J.sw, 32) * cdiv(J.sh, 8) : 0;
     case S_DET_MAP: return (J.guided && J.algo == 6 && J.detailFused) ? cdiv(J.sw, kDetailTile) * cdiv(J.sh, J.detailRows) : 0;
@@ -987,6 +991,19 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_YC, k_yc_h, b32x8);
     go(S_YC_TILED, k_yc_tiled, b32x8);
     go(S_AFFINE, k_affine, b32x8);
+    if (plan.totals[S_AFFINE_LIST] > 0) {
+        // persistent grid over the algo 6 frames' chroma lists
+        static int gridBlocks = 0;
+        if (gridBlocks == 0) {
+            int dev = 0, sms = 0, perSm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_affine_list, 256, 0);
+            gridBlocks = std::max(1, sms * std::max(1, perSm));
+        }
+        k_affine_list<<<gridBlocks, 256, 0, stream>>>(dJobs, pre(S_AFFINE_LIST), n);
+        ++launches;
+    }
     go(S_DET_HPASS, k_detail_hpass, b32x8);
     go(S_DET_PLAIN, k_detail_plain, b32x8);
     go(S_DET_MAP, k_detail_map, b32x8);

@@ -116,6 +116,7 @@ struct __align__(16) FrameJob {
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
     int xferListed;                    // algo 6: detail transfer walks the work list
+    uint32_t *chromaList;              // algo 6 sparse: active chroma samples (y << 16 | x)
     int bumpRcpSafe;                   // every guided bump denominator stays below 2^64
     int plainFused;                    // k_plain computes its horizontal rows itself
     int plainRows;                     // output rows per k_plain block
