@@ -718,6 +718,10 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     __shared__ float src[3][SH][SW];
     __shared__ GateTile T;
     __shared__ FrameJob sJob;
+    __shared__ int sActive;
+    static_assert(sizeof(src) >= GT_X * GT_Y * sizeof(uint16_t), "sample list fits the staged samples");
+    // the active-sample list reuses the staged samples once the gradients exist
+    uint16_t *sList = reinterpret_cast<uint16_t *>(&src[0][0][0]);
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     stageJob(jobs, f, sJob);
     const FrameJob &J = sJob;
@@ -776,18 +780,38 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
             T.guv[r][c] = make_float4(g[2], g[4], g[3], g[5]);
         }
     }
+    // the tile's active samples, compacted so every thread takes a share
+    // (inactive samples store the sparse plane's zeros here); the barrier also
+    // ends the gradient pass's reads of the staged samples
+    if (tx == 0 && ty == 0)
+        sActive = 0;
     __syncthreads();
     const int x = x0 + tx;
-    if (x >= w)
-        return;
-    const bool interior = x0 >= GH && y0 >= GH && x0 + GT_X + GH <= w && y0 + GT_Y + GH <= h;
-    for (int y = y0 + ty; y < min(y0 + GT_Y, h); y += 8) {
-        const size_t o = (size_t)y * w + x;
-        if (!dense && J.cmask[o] == 0) {
-            J.ms[o] = 0.0f;
-            continue;
+    for (int r = ty; r < GT_Y; r += 8) {
+        const int y = y0 + r;
+        bool on = false;
+        if (x < w && y < h) {
+            const size_t o = (size_t)y * w + x;
+            on = dense || J.cmask[o] != 0;
+            if (!on)
+                J.ms[o] = 0.0f;
         }
-        J.ms[o] = interior ? gateAt<true>(T, x, y, x0, y0, w, h) : gateAt<false>(T, x, y, x0, y0, w, h);
+        const uint32_t ballot = __ballot_sync(0xffffffffu, on);
+        int base = 0;
+        if (tx == 0 && ballot)
+            base = atomicAdd(&sActive, __popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (on)
+            sList[base + __popc(ballot & ((1u << tx) - 1u))] = (uint16_t)(r * GT_X + tx);
+    }
+    __syncthreads();
+    const bool interior = x0 >= GH && y0 >= GH && x0 + GT_X + GH <= w && y0 + GT_Y + GH <= h;
+    const int count = sActive;
+    for (int i = ty * GT_X + tx; i < count; i += GT_X * 8) {
+        const int e = sList[i];
+        const int sx = x0 + (e % GT_X), sy = y0 + e / GT_X;
+        J.ms[(size_t)sy * w + sx] =
+            interior ? gateAt<true>(T, sx, sy, x0, y0, w, h) : gateAt<false>(T, sx, sy, x0, y0, w, h);
     }
 }
 
