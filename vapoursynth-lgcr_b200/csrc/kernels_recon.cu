@@ -267,6 +267,17 @@ __device__ __forceinline__ void plainFromStaged(const FrameJob &J, const float2 
     outV = (float)vV;
 }
 
+// Position of the n-th (0-based) set bit of m (n < popc(m)): the largest p
+// with fewer than n + 1 set bits below p.
+__device__ __forceinline__ int nthSetBit(uint32_t m, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1)
+        if (__popc(m & ((1u << (pos + s)) - 1u)) <= n)
+            pos += s;
+    return pos;
+}
+
 // Per-row vertical tap data of one k_plain block, staged once for the
 // block's output rows (at most kPlainRows; supports up to 8 taps).
 struct PlainRows {
@@ -430,6 +441,7 @@ k_plain(LGCR_STAGE_ARGS) {
         plainRowsSmem + size_t(kPlainStagedRows) * 32 * 24);
     __shared__ PlainRows R;
     __shared__ FrameJob sJob;
+    __shared__ uint32_t sRowBits[8][kPlainRows / 8];   // per warp: plain pixels of its rows
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     stageJob(jobs, f, sJob);
     const FrameJob &J = sJob;
@@ -502,14 +514,85 @@ k_plain(LGCR_STAGE_ARGS) {
         }
     }
     __syncthreads();
-    if (ox >= J.W)
-        return;
+    const bool colValid = ox < J.W;
     float wsX = 0.0f, waX = 0.0f, posX = 0.0f;
-    if (rowTables) {
+    if (rowTables && colValid) {
         wsX = __ldg(J.ax.wsum + ox);
         waX = __ldg(J.ax.wabs + ox);
         posX = __ldg(J.ax.pos + ox);
     }
+    if (skipListed && rowTables) {
+        // Listed pixels only fold extrema here; the warp's plain pixels over
+        // its rows (threadIdx.y + 8m) are compacted so full warps evaluate them.
+        uint32_t *rowBits = sRowBits[threadIdx.y];
+        int total = 0;
+        for (int m = 0; m < kPlainRows / 8; ++m) {
+            const int k = threadIdx.y + 8 * m;
+            bool plainPx = false;
+            if (k < rowsHere && colValid) {
+                const int oy = oy0 + k;
+                const bool act = maskWords ? ((R.maskWord[k] >> lx) & 1u) != 0 : pixelActive(J, ox, oy);
+                if (act && foldExtrema) {
+                    const size_t o = (size_t)oy * J.W + ox;
+                    if (J.noClampY) {
+                        switch (sup) {
+                        case 4: extremaFromRows<4, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                        case 6: extremaFromRows<6, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                        default: extremaFromRows<8, true>(J, sE, sL, R, k, syLo, lx, o); break;
+                        }
+                    } else {
+                        switch (sup) {
+                        case 4: extremaFromRows<4, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                        case 6: extremaFromRows<6, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                        default: extremaFromRows<8, false>(J, sE, sL, R, k, syLo, lx, o); break;
+                        }
+                    }
+                }
+                plainPx = !act;
+            }
+            const uint32_t b = __ballot_sync(0xffffffffu, plainPx);
+            if (lx == 0)
+                rowBits[m] = b;
+            total += __popc(b);
+        }
+        __syncwarp();
+        for (int base = 0; base < total; base += 32) {
+            const int j = base + lx;
+            int m = 0, col = 0, before = 0;
+            if (j < total) {
+                uint32_t b = rowBits[0];
+                while (before + __popc(b) <= j) {
+                    before += __popc(b);
+                    b = rowBits[++m];
+                }
+                col = nthSetBit(b, j - before);
+            }
+            const float wsC = __shfl_sync(0xffffffffu, wsX, col);
+            const float waC = __shfl_sync(0xffffffffu, waX, col);
+            const float posC = __shfl_sync(0xffffffffu, posX, col);
+            if (j < total) {
+                const int k = threadIdx.y + 8 * m;
+                float u, v;
+                if (J.noClampY) {
+                    switch (sup) {
+                    case 4: plainFromRows<4, true>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    case 6: plainFromRows<6, true>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    default: plainFromRows<8, true>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    }
+                } else {
+                    switch (sup) {
+                    case 4: plainFromRows<4, false>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    case 6: plainFromRows<6, false>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    default: plainFromRows<8, false>(J, sHV, sE, R, k, syLo, col, wsC, waC, posC, u, v); break;
+                    }
+                }
+                emit(J, colBase + col, oy0 + k, u, v);
+            }
+        }
+        return;
+    }
+    if (!colValid)
+        return;
     for (int k = threadIdx.y; k < rowsHere; k += blockDim.y) {
         const int oy = oy0 + k;
         // listed pixels of algo 2 and integer algo 4 are written by k_guided
