@@ -50,16 +50,18 @@ struct HColumn {
     }
 };
 
-template <int SUP, bool NOCLAMP>
+// LUMA: also the extrema of lc (read only by the guided pass: the folded
+// window extrema or the horizontal table).
+template <int SUP, bool NOCLAMP, bool LUMA = true>
 __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &col, int sy, float4 &ea,
                                        float4 &eb) {
     const int cw = J.cw;
     const size_t row = (size_t)sy * cw;
     const double2 *uv = reinterpret_cast<const double2 *>(J.uvd) + row;
-    const float *urow = J.U + row, *vrow = J.V + row;
-    const float *lrow = J.lc ? J.lc + row : nullptr;
+    const float *lrow = (LUMA && J.lc) ? J.lc + row : nullptr;
     double hU = 0.0, hV = 0.0;
-    // extrema of the float samples (the doubles hold the same values)
+    // extrema of the float samples: the doubles hold them exactly, so they
+    // narrow back without a second load
     float mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
     float mnL = 1e30f, mxL = -1e30f;
 #pragma unroll
@@ -71,10 +73,10 @@ __device__ __forceinline__ void hEntry(const FrameJob &J, const HColumn<SUP> &co
         const double w = col.w[i];
         hU = fma(w, p.x, hU);
         hV = fma(w, p.y, hV);
-        const float u = ldf(urow + x), v = ldf(vrow + x);
+        const float u = (float)p.x, v = (float)p.y;
         mnU = runMin(mnU, u); mxU = runMax(mxU, u);
         mnV = runMin(mnV, v); mxV = runMax(mxV, v);
-        if (lrow) {
+        if (LUMA && lrow) {
             const float l = ldf(lrow + x);
             mnL = runMin(mnL, l); mxL = runMax(mxL, l);
         }
@@ -353,7 +355,7 @@ __device__ __forceinline__ void putEntry(const FrameJob &J, int ox, int lx, int 
         storeEntry(J, ox, sy, a, b);
 }
 
-template <int SUP, bool NOCLAMP>
+template <int SUP, bool NOCLAMP, bool LUMA>
 __device__ __forceinline__ void stageRowsT(const FrameJob &J, const HColumn<SUP> &col, int ox, int lx,
                                            int syLo, int nRows, int syOwnEnd, bool writeTable,
                                            const PlainStage &s) {
@@ -361,14 +363,14 @@ __device__ __forceinline__ void stageRowsT(const FrameJob &J, const HColumn<SUP>
     int r = threadIdx.y;
     for (; r + step < nRows; r += 2 * step) {
         float4 a0, b0, a1, b1;
-        hEntry<SUP, NOCLAMP>(J, col, syLo + r, a0, b0);
-        hEntry<SUP, NOCLAMP>(J, col, syLo + r + step, a1, b1);
+        hEntry<SUP, NOCLAMP, LUMA>(J, col, syLo + r, a0, b0);
+        hEntry<SUP, NOCLAMP, LUMA>(J, col, syLo + r + step, a1, b1);
         putEntry(J, ox, lx, r, syLo + r, a0, b0, syOwnEnd, writeTable, s);
         putEntry(J, ox, lx, r + step, syLo + r + step, a1, b1, syOwnEnd, writeTable, s);
     }
     if (r < nRows) {
         float4 a, b;
-        hEntry<SUP, NOCLAMP>(J, col, syLo + r, a, b);
+        hEntry<SUP, NOCLAMP, LUMA>(J, col, syLo + r, a, b);
         putEntry(J, ox, lx, r, syLo + r, a, b, syOwnEnd, writeTable, s);
     }
 }
@@ -378,10 +380,18 @@ __device__ __forceinline__ void stageRows(const FrameJob &J, int ox, int lx, int
                                           int syOwnEnd, bool writeTable, const PlainStage &s) {
     HColumn<SUP> col;
     col.load(J.ax, ox);
-    if (J.noClampX)
-        stageRowsT<SUP, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
-    else
-        stageRowsT<SUP, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
+    // the luma extrema only feed the guided pass (folded planes or the table)
+    if (J.wLum || writeTable) {
+        if (J.noClampX)
+            stageRowsT<SUP, true, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
+        else
+            stageRowsT<SUP, false, true>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
+    } else {
+        if (J.noClampX)
+            stageRowsT<SUP, true, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
+        else
+            stageRowsT<SUP, false, false>(J, col, ox, lx, syLo, nRows, syOwnEnd, writeTable, s);
+    }
 }
 
 __device__ __forceinline__ void stageRowsGeneric(const FrameJob &J, int ox, int lx, int syLo, int nRows,
