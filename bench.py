@@ -276,7 +276,7 @@ def serve_requests(n, seed=4000):
              int(rng.choice([2, 4, 6])), bool(rng.random() < 0.1)) for _ in range(n)]
 
 
-def serving_leg(frames, n_requests, lanes=4, max_batch=8, budget=8 << 30):
+def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30):
     """Poisson arrivals at 1.2x the per-frame path's capacity into the
     continuous-batching server; latency from submit to completion on the
     server's clock."""
@@ -645,7 +645,7 @@ def main():
                          "flight); default: the host's cores, at most 16, as the reference arm")
     ap.add_argument("--serve-requests", type=int, default=4000,
                     help="requests of the serving leg (0 skips it)")
-    ap.add_argument("--serve-lanes", type=int, default=4,
+    ap.add_argument("--serve-lanes", type=int, default=2,
                     help="concurrent device batches of the serving leg")
     ap.add_argument("--batch-only", action="store_true",
                     help="time the batched form only (profiler captures)")
