@@ -6,13 +6,15 @@
 //   k_plain   plain base per output pixel: vertical pass over the table
 //             (separable, src/recon.cpp:1281-1437), bilinear
 //             (src/recon.cpp:1031-1149) or radial (src/recon.cpp:828-1029);
-//             writes the final sample of pixels the guided pass skips
+//             writes the final sample of pixels the guided pass skips and,
+//             for the pixels it lists, folds their guided windows' extrema
 //   k_guided  reconstructChromaImpl (scalar, src/recon.cpp:14-819) for the
 //             active pixels of every frame in the launch: a persistent grid
 //             walks the frames' compacted work lists (no divergence between
 //             plain and guided pixels). Pass 1 (window luma range and chroma
-//             hull) reads the horizontal table; pass 2 is specialized on the
-//             tap support so per-column terms stay in registers.
+//             hull) reads the extrema k_plain folded (or the horizontal
+//             table); pass 2 is specialized on the tap support so per-column
+//             terms stay in registers.
 //   luma resize       resampleH/V, resampleRadial src/kernels.cpp:171-334
 //   output store      floatToPlane src/lgcr.h:997-1013
 // FP64 accumulators stay FP64 (B200 issues FP64 at half the FP32 rate); a
@@ -440,7 +442,10 @@ __device__ __forceinline__ void extremaFromRows(const FrameJob &J, const float4 
 //  * other frames stage rows of the table written by k_hpass, or read the
 //    table directly when the rows do not fit (strong vertical downscale).
 // The vertical pass then runs from shared memory, with the per-row tap data
-// and active-pixel bits staged once per block for supports up to 8.
+// and active-pixel bits staged once per block for supports up to 8. Pixels
+// the guided pass lists get their window extrema folded instead (frames
+// with extrema planes), and each warp compacts its remaining plain pixels
+// across its rows so full warps evaluate them.
 __global__ void __launch_bounds__(256, 4)
 k_plain(LGCR_STAGE_ARGS) {
     extern __shared__ __align__(16) unsigned char plainRowsSmem[];
