@@ -30,6 +30,14 @@ cudaStream_t threadStream() {
     return s;
 }
 
+// Completion event of the calling thread's frames (blocking sync), or null.
+cudaEvent_t threadDoneEvent() {
+    thread_local cudaEvent_t ev = nullptr;
+    if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess)
+        ev = nullptr;
+    return ev;
+}
+
 bool checkPlane(const lgcr_plane &p, int w, int h, int bps, bool allowNull) {
     if (!p.data)
         return allowNull;
@@ -178,8 +186,14 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
     ws->used = true;
     const FrameJob J = *ws->hJob;
     F.release(ws);
-    if (e == cudaSuccess && (memory == LGCR_MEM_HOST || stats))
-        e = cudaStreamSynchronize(s);
+    // wait on a blocking-sync event of this thread recorded after the frame's
+    // last operation: the calling thread sleeps instead of spinning on a core
+    if (e == cudaSuccess && (memory == LGCR_MEM_HOST || stats)) {
+        const cudaEvent_t fin = threadDoneEvent();
+        e = fin ? cudaEventRecord(fin, s) : cudaStreamSynchronize(s);
+        if (fin && e == cudaSuccess)
+            e = cudaEventSynchronize(fin);
+    }
     if (e != cudaSuccess)
         return cudaFail(e, "lgcr_recon_frame");
     if (stats) {
