@@ -1037,7 +1037,8 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     const bool rcpSafe = J.bumpRcpSafe && (1.0f + maxAbsDL * maxAbsDL * invSigma2) < kRcpFastLimit;
     const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
     if (fast && ax.sup == 8)
-        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, maskBits(amx, 8), maskBits(amy, 8), a);
+        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, ax.amBits ? __ldg(ax.amBits + ox) : maskBits(amx, 8),
+                         ay.amBits ? __ldg(ay.amBits + oy) : maskBits(amy, 8), a);
     else if (fast && ax.sup == 6)
         tapsSeparable<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
     else if (fast && ax.sup == 4)

@@ -221,7 +221,7 @@ struct Packer {
     }
 };
 
-struct AxisOffsets { size_t start, w, wd, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF, kmx, kss; int n, sup; };
+struct AxisOffsets { size_t start, w, wd, am, wsum, wabs, pos, lpos, cbI0, cbF, lbI0, lbF, kmx, kss, amBits; int n, sup; };
 
 AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
     AxisOffsets o;
@@ -235,6 +235,13 @@ AxisOffsets packAxis(Packer &pk, const ChromaAxis &a) {
     std::vector<float> kmx, kss;
     rescueFactors(a, kmx, kss);
     o.kmx = pk.add(kmx); o.kss = pk.add(kss);
+    // tap activity of each index as one word (the same bits as the bytes)
+    std::vector<uint32_t> bits(a.sup <= 32 ? size_t(a.n) : 0, 0u);
+    for (size_t i = 0; i < bits.size(); ++i)
+        for (int j = 0; j < a.sup; ++j)
+            if (a.am[i * a.sup + j])
+                bits[i] |= 1u << j;
+    o.amBits = pk.add(bits);
     return o;
 }
 
@@ -249,6 +256,7 @@ AxisView axisView(const DeviceArena &ar, const AxisOffsets &o) {
     v.cbF = (const float *)ar.at(o.cbF); v.lbI0 = (const int *)ar.at(o.lbI0);
     v.lbF = (const float *)ar.at(o.lbF);
     v.kmx = (const float *)ar.at(o.kmx); v.kss = (const float *)ar.at(o.kss);
+    v.amBits = o.sup <= 32 ? (const uint32_t *)ar.at(o.amBits) : nullptr;
     return v;
 }
 

@@ -34,6 +34,7 @@ struct AxisView {
     const int *cbI0, *lbI0;
     const float *cbF, *lbF;
     const float *kmx, *kss;  // rescue kappa factors per index (separable kernels)
+    const uint32_t *amBits;  // per index: bit i set when tap i is active (sup <= 32), or null
 };
 
 struct RadialView {

@@ -180,6 +180,7 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
         v.lbF = (const float *)(base + o.lf);
         v.kmx = (const float *)(base + o.kmx);
         v.kss = (const float *)(base + o.kss);
+        v.amBits = nullptr;      // activity read from the bytes
         return v;
     };
     T.ax = axisView(oa[0], ax);
