@@ -739,13 +739,26 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
                                               const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
     constexpr int NP = SUP / 2;
     f32x2 dxnx[NP], dxny[NP], wxv[NP];
+    if (SUP % 4 == 0) {
+        // the column's weights as 16-byte loads (rows of SUP floats in a
+        // 256-byte aligned table)
+#pragma unroll
+        for (int q = 0; q < NP; q += 2) {
+            const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wxp) + q / 2);
+            wxv[q] = pk2(w4.x, w4.y);
+            wxv[q + 1] = pk2(w4.z, w4.w);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+            wxv[q] = pk2(__ldg(wxp + 2 * q), __ldg(wxp + 2 * q + 1));
+    }
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
         const float dx0 = ((float)(tx0 + 2 * q) - c.scx) * c.rwF;
         const float dx1 = ((float)(tx0 + 2 * q + 1) - c.scx) * c.rwF;
         dxnx[q] = pk2(dx0 * c.nx, dx1 * c.nx);
         dxny[q] = pk2(-dx0 * c.ny, -dx1 * c.ny);
-        wxv[q] = pk2(__ldg(wxp + 2 * q), __ldg(wxp + 2 * q + 1));
     }
     const f32x2 one = pk2(1.0f, 1.0f);
     const f32x2 L0 = pk2(c.L0, c.L0), invS = pk2(c.invSigma2, c.invSigma2);
