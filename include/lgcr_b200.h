@@ -165,7 +165,10 @@ const char *lgcr_last_error(void);
  * message. The first call on a device looks up the array's address and
  * should come before any stream capture. All calls share the array: calls
  * whose work overlaps on the GPU race and must be ordered by the caller.
- * Work is enqueued on `stream` (a cudaStream_t); the call does not wait.
+ * Work is enqueued on `stream` (a cudaStream_t) and the call does not wait
+ * for the GPU to run it; its uploads of the geometry tables and the frame
+ * descriptor read pageable host memory, so the call may block the host until
+ * those few kilobytes are staged.
  */
 int lgcr_recon_frame_static(lgcr_recon *filter, const lgcr_plane in[3],
                             const lgcr_plane out[3], int chroma_location, void *stream);

@@ -1,6 +1,14 @@
-"""lgcr_recon_frame_static (the entry point that allocates no device memory,
-for callers that cannot call cudaMalloc) against lgcr_recon_frame on the
-same frames, two calls in a row, through the C ABI. Collected last."""
+"""lgcr_recon_frame_static, the entry point that allocates no device memory.
+
+Some callers cannot call cudaMalloc: hosts that hand every byte of device
+memory out of their own pool, and latency-critical paths where an allocation
+would synchronize the device. This file checks the entry point through the C
+ABI against lgcr_recon_frame and against the oracle (the reference's scalar
+build) on the same frames, two calls in a row, including frames whose chroma
+planes are narrower than the kernel support (the clamped-tap path), and
+checks that a call on a fresh filter leaves the device's free memory
+unchanged. Collected last, so a run that stops at the first failure has run
+every other test before it."""
 import ctypes
 
 import numpy as np
@@ -16,6 +24,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 import lgcr
 from lgcr import synthetic as S
+from oracle import oracle as O
 
 
 def bind():
@@ -37,17 +46,29 @@ def to_device(planes):
     return out
 
 
+def to_host(planes):
+    return [p.cpu().numpy() if p.dtype != torch.uint16
+            else p.view(torch.int16).cpu().numpy().view(np.uint16) for p in planes]
+
+
 def empty_like_out(rec, dev_planes):
     return [torch.empty((rec.out_h, rec.out_w), dtype=dev_planes[0].dtype, device="cuda")
             for _ in range(3)]
 
 
-@pytest.mark.parametrize("fmt,geom,kw", [
+CASES = [
     (S.YUV420P10, (640, 360), dict(algo=2, kernel="lanczos", taps=4)),
     (S.YUV420PS, (320, 180), dict(algo=2, kernel="jinc", taps=3, width=480, height=270)),
     (S.YUV422P10, (256, 144), dict(algo=6, strength=0.0, kernel="spline36")),
-])
-def test_static_matches_regular_twice(fmt, geom, kw):
+    # chroma planes narrower/shorter than the tap support: clamped tap indices
+    (S.YUV420P10, (8, 8), dict(algo=2, kernel="lanczos", taps=4)),
+    (S.YUV420P8, (12, 10), dict(algo=2, kernel="spline36", sparse=0)),
+    (S.YUV422P10, (16, 12), dict(algo=2, kernel="lanczos", taps=3)),
+]
+
+
+@pytest.mark.parametrize("fmt,geom,kw", CASES)
+def test_static_matches_regular_and_oracle_twice(fmt, geom, kw):
     lib, fn = bind()
     w, h = geom
     rec = lgcr.Recon(lgcr.video_format(w, h, fmt.bits, fmt.ssw, fmt.ssh), **kw)
@@ -61,10 +82,35 @@ def test_static_matches_regular_twice(fmt, geom, kw):
         status = fn(rec.handle, lgcr.planes_desc(dev), lgcr.planes_desc(got), -1, stream)
         assert status == 0, lib.lgcr_last_error().decode()
         torch.cuda.synchronize()
-        host = lambda planes_: [p.cpu().numpy() if p.dtype != torch.uint16
-                                else p.view(torch.int16).cpu().numpy().view(np.uint16)
-                                for p in planes_]
-        assert_parity(host(got), host(ref), fmt.is_float, f"static call {call}")
+        assert_parity(to_host(got), to_host(ref), fmt.is_float, f"static vs regular, call {call}")
+        oracle, _ = O.Recon(O.make_format(planes, fmt.bits), "scalar", **kw).frame(planes)
+        assert_parity(to_host(got), oracle, fmt.is_float, f"static vs oracle, call {call}")
+
+
+def test_static_call_allocates_no_device_memory():
+    lib, fn = bind()
+    fmt = S.YUV420P10
+    w, h = 320, 192
+    kw = dict(algo=2, kernel="lanczos", taps=4)
+    stream = torch.cuda.current_stream().cuda_stream
+    planes = S.make_frame(w, h, fmt, seed=90)
+    dev = to_device(planes)
+    # a first call loads the library's kernels and resolves the scratch array
+    warm = lgcr.Recon(lgcr.video_format(w, h, 10, 1, 1), **kw)
+    outs = empty_like_out(warm, dev)
+    assert fn(warm.handle, lgcr.planes_desc(dev), lgcr.planes_desc(outs), -1, stream) == 0
+    torch.cuda.synchronize()
+    fresh = lgcr.Recon(lgcr.video_format(w, h, 10, 1, 1), **kw)
+    got = empty_like_out(fresh, dev)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        assert fn(fresh.handle, lgcr.planes_desc(dev), lgcr.planes_desc(got), -1, stream) == 0
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, f"device free memory changed by {free_before - free_after} B"
+    oracle, _ = O.Recon(O.make_format(planes, 10), "scalar", **kw).frame(planes)
+    assert_parity(to_host(got), oracle, False, "static on a fresh filter vs oracle")
 
 
 def test_static_rejects_oversize_and_unsupported():

@@ -151,6 +151,12 @@ struct Filter {
 int createFilter(const lgcr_params *params, const lgcr_format *fmt, Filter **out,
                  std::string &err);
 
+// Scalar geometry of a table set that every builder must fill the same way:
+// the chroma axes' supports (they decide buildJob's unclamped-tap and fast
+// reciprocal flags) and the k_plain block height.
+void setAxisGeometry(DeviceTables &t, const ChromaAxis &ax, const ChromaAxis &ay, int outH,
+                     int ch);
+
 // Fill the device FrameJob of one task.
 void buildJob(const FrameTask &t, FrameJob &job);
 

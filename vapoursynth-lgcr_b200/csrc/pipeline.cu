@@ -292,6 +292,33 @@ RadialView radialView(const DeviceArena &ar, const RadialOffsets &o) {
 
 } // namespace
 
+void setAxisGeometry(DeviceTables &t, const ChromaAxis &ax, const ChromaAxis &ay, int outH,
+                     int ch) {
+    t.axSup = ax.sup;
+    t.aySup = ay.sup;
+    // k_plain blocks: tall when every block's chroma rows fit in shared memory
+    auto plainRowsRead = [&](int rows) {
+        int most = 0;
+        for (int oy0 = 0; oy0 < outH; oy0 += rows) {
+            const int oyLast = std::min(oy0 + rows, outH) - 1;
+            const int lo = std::clamp(ay.start[oy0], 0, ch - 1);
+            const int hi = std::clamp(ay.start[oyLast] + ay.sup - 1, 0, ch - 1);
+            most = std::max(most, hi - lo + 1);
+        }
+        return most;
+    };
+    t.plainRows = kPlainRowsShort;
+    t.plainMaxRows = plainRowsRead(kPlainRowsShort);
+    for (int rows = kPlainRows; rows > kPlainRowsShort; rows -= 8) {
+        const int most = plainRowsRead(rows);
+        if (most <= kPlainStagedRows) {
+            t.plainRows = rows;
+            t.plainMaxRows = most;
+            break;
+        }
+    }
+}
+
 const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
     std::lock_guard<std::mutex> lock(mu);
     for (auto &t : tables)
@@ -405,29 +432,7 @@ const DeviceTables *Filter::tablesFor(double shiftX, double shiftY) {
         return nullptr;
     t->ax = axisView(t->arena, oax);
     t->ay = axisView(t->arena, oay);
-    t->axSup = ax.sup;
-    t->aySup = ay.sup;
-    // k_plain blocks: tall when every block's chroma rows fit in shared memory
-    auto plainRowsRead = [&](int rows) {
-        int most = 0;
-        for (int oy0 = 0; oy0 < p.outH; oy0 += rows) {
-            const int oyLast = std::min(oy0 + rows, p.outH) - 1;
-            const int lo = std::clamp(ay.start[oy0], 0, ch - 1);
-            const int hi = std::clamp(ay.start[oyLast] + ay.sup - 1, 0, ch - 1);
-            most = std::max(most, hi - lo + 1);
-        }
-        return most;
-    };
-    t->plainRows = kPlainRowsShort;
-    t->plainMaxRows = plainRowsRead(kPlainRowsShort);
-    for (int rows = kPlainRows; rows > kPlainRowsShort; rows -= 8) {
-        const int most = plainRowsRead(rows);
-        if (most <= kPlainStagedRows) {
-            t->plainRows = rows;
-            t->plainMaxRows = most;
-            break;
-        }
-    }
+    setAxisGeometry(*t, ax, ay, p.outH, ch);
     if (p.k.radial)
         t->rad = radialView(t->arena, orad);
     if (!sameSize && !p.k.radial) {

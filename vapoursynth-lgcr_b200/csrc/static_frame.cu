@@ -185,6 +185,7 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
     };
     T.ax = axisView(oa[0], ax);
     T.ay = axisView(oa[1], ay);
+    setAxisGeometry(T, ax, ay, q.outH, F.ch);
     if (q.k.radial) {
         T.rad.valid = rad.valid;
         T.rad.supX = rad.supportX; T.rad.supY = rad.supportY; T.rad.phasesX = rad.phaseCountX;
