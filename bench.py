@@ -34,6 +34,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -84,11 +85,11 @@ class Clocks:
     def __init__(self, index=0):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        fd, self.path = tempfile.mkstemp(prefix=f"lgcr_clocks_rank{index}_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
@@ -112,7 +113,9 @@ class Clocks:
 
     def summary(self):
         try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            with open(self.path) as fh:
+                rows = [r.split(",") for r in fh.read().strip().splitlines() if r.strip()]
+            os.unlink(self.path)
         except Exception:
             return None
         rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
