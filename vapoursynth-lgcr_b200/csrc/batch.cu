@@ -2,7 +2,10 @@
 // depths) per launch of each stage. The launch sequence of a batch layout is
 // captured once into a CUDA graph and replayed; per-frame descriptors and
 // stage prefix tables are refreshed by copy nodes that read pinned host
-// buffers, so new frames (new plane pointers) replay the same graph.
+// buffers, so new frames (new plane pointers) replay the same graph. Runs
+// rotate over a few descriptor slots (each with its graph), so a call waits
+// only for the run that used its slot several calls earlier, not for the
+// previous one.
 #include "impl.h"
 #include "kernels.cuh"
 
@@ -16,16 +19,36 @@ struct StageEvent {
     cudaEvent_t start, stop;
 };
 
-struct lgcr_batch {
-    int capacity = 0;
+// Descriptor buffers of one in-flight run: pinned host copies the run's
+// copy nodes read, their device targets, and the event that marks them read.
+// A batch cycles through kDescriptorSlots of them, so the host prepares the
+// next run while the previous one executes; each slot keeps its own graph.
+struct DescriptorSlot {
     FrameJob *dJobs = nullptr, *hJobs = nullptr;
     int *dPrefix = nullptr, *hPrefix = nullptr;
-    size_t prefixCapacity = 0;
     cudaEvent_t done = nullptr;
     bool pending = false;
-    // graph cache (one layout)
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec = nullptr;     // graph of the cached layout on this slot
     std::string signature;
+    int launches = 0;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (dJobs) cudaFree(dJobs);
+        if (hJobs) cudaFreeHost(hJobs);
+        if (dPrefix) cudaFree(dPrefix);
+        if (hPrefix) cudaFreeHost(hPrefix);
+        exec = nullptr; dJobs = nullptr; hJobs = nullptr; dPrefix = nullptr; hPrefix = nullptr;
+        signature.clear();
+    }
+};
+
+constexpr int kDescriptorSlots = 3;
+
+struct lgcr_batch {
+    int capacity = 0;
+    size_t prefixCapacity = 0;
+    DescriptorSlot slots[kDescriptorSlots];
+    int next = 0;                       // slot of the next run
     int lastLaunches = 0;
     // profiling
     bool profiling = false;
@@ -34,12 +57,10 @@ struct lgcr_batch {
     std::vector<double> stageMs;
     std::vector<int> stageLaunches;
     ~lgcr_batch() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (dJobs) cudaFree(dJobs);
-        if (hJobs) cudaFreeHost(hJobs);
-        if (dPrefix) cudaFree(dPrefix);
-        if (hPrefix) cudaFreeHost(hPrefix);
-        if (done) cudaEventDestroy(done);
+        for (auto &sl : slots) {
+            sl.release();
+            if (sl.done) cudaEventDestroy(sl.done);
+        }
         for (auto &e : events) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
         for (auto e : eventPool) cudaEventDestroy(e);
     }
@@ -61,36 +82,42 @@ cudaEvent_t poolEvent(lgcr_batch *b) {
 int ensureCapacity(lgcr_batch *b, int count) {
     if (count <= b->capacity && size_t(stageCount()) * (count + 1) <= b->prefixCapacity)
         return LGCR_OK;
-    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->signature.clear(); }
-    if (b->dJobs) cudaFree(b->dJobs);
-    if (b->hJobs) cudaFreeHost(b->hJobs);
-    if (b->dPrefix) cudaFree(b->dPrefix);
-    if (b->hPrefix) cudaFreeHost(b->hPrefix);
+    for (auto &sl : b->slots) {
+        if (sl.pending)
+            cudaEventSynchronize(sl.done);
+        sl.pending = false;
+        sl.release();
+    }
     const int cap = std::max(count, 8);
     b->prefixCapacity = size_t(stageCount()) * (cap + 1);
-    if (cudaMalloc(&b->dJobs, sizeof(FrameJob) * cap) != cudaSuccess ||
-        cudaHostAlloc((void **)&b->hJobs, sizeof(FrameJob) * cap, cudaHostAllocDefault) != cudaSuccess ||
-        cudaMalloc(&b->dPrefix, b->prefixCapacity * sizeof(int)) != cudaSuccess ||
-        cudaHostAlloc((void **)&b->hPrefix, b->prefixCapacity * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
-        setError("LGCR: batch descriptor allocation failed");
-        return LGCR_E_NOMEM;
+    for (auto &sl : b->slots) {
+        if (cudaMalloc(&sl.dJobs, sizeof(FrameJob) * cap) != cudaSuccess ||
+            cudaHostAlloc((void **)&sl.hJobs, sizeof(FrameJob) * cap, cudaHostAllocDefault) != cudaSuccess ||
+            cudaMalloc(&sl.dPrefix, b->prefixCapacity * sizeof(int)) != cudaSuccess ||
+            cudaHostAlloc((void **)&sl.hPrefix, b->prefixCapacity * sizeof(int), cudaHostAllocDefault) !=
+                cudaSuccess) {
+            for (auto &other : b->slots)
+                other.release();
+            b->capacity = 0;
+            b->prefixCapacity = 0;
+            setError("LGCR: batch descriptor allocation failed");
+            return LGCR_E_NOMEM;
+        }
     }
     b->capacity = cap;
     return LGCR_OK;
 }
 
 // Launch sequence; with profiling, each launched stage is bracketed by events.
-int enqueue(lgcr_batch *b, const std::vector<FrameJob> &jobs, const StagePlan &plan,
-            cudaStream_t s, bool copies) {
+int enqueue(lgcr_batch *b, DescriptorSlot &sl, const std::vector<FrameJob> &jobs,
+            const StagePlan &plan, cudaStream_t s) {
     const int n = int(jobs.size());
-    if (copies) {
-        if (cudaMemcpyAsync(b->dJobs, b->hJobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-            cudaMemcpyAsync(b->dPrefix, b->hPrefix, plan.prefix.size() * sizeof(int),
-                            cudaMemcpyHostToDevice, s) != cudaSuccess)
-            return -1;
-    }
+    if (cudaMemcpyAsync(sl.dJobs, sl.hJobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(sl.dPrefix, sl.hPrefix, plan.prefix.size() * sizeof(int),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return -1;
     if (!b->profiling)
-        return launchStages(jobs, plan, b->dJobs, b->dPrefix, s);
+        return launchStages(jobs, plan, sl.dJobs, sl.dPrefix, s);
     // profiled: one stage at a time so each launch gets its own events
     int launches = 0;
     StagePlan single = plan;
@@ -101,7 +128,7 @@ int enqueue(lgcr_batch *b, const std::vector<FrameJob> &jobs, const StagePlan &p
             single.totals[o] = (o == st) ? plan.totals[st] : 0;
         StageEvent ev{st, poolEvent(b), poolEvent(b)};
         cudaEventRecord(ev.start, s);
-        const int l = launchStages(jobs, single, b->dJobs, b->dPrefix, s);
+        const int l = launchStages(jobs, single, sl.dJobs, sl.dPrefix, s);
         cudaEventRecord(ev.stop, s);
         if (l < 0)
             return -1;
@@ -119,8 +146,9 @@ int lgcr_batch_create(lgcr_batch **out) {
     if (!out)
         return LGCR_E_ARGUMENT;
     auto b = std::make_unique<lgcr_batch>();
-    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
-        return cudaFail(cudaGetLastError(), "lgcr_batch_create");
+    for (auto &sl : b->slots)
+        if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
+            return cudaFail(cudaGetLastError(), "lgcr_batch_create");
     b->stageMs.assign(stageCount(), 0.0);
     b->stageLaunches.assign(stageCount(), 0);
     *out = b.release();
@@ -146,9 +174,12 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
     int status = ensureCapacity(b, count);
     if (status != LGCR_OK)
         return status;
-    // the pinned descriptors are rewritten: the previous run must have read them
-    if (b->pending)
-        cudaEventSynchronize(b->done);
+    // this run's pinned descriptors are rewritten: the run that last used the
+    // slot (kDescriptorSlots runs ago) must have read them
+    DescriptorSlot &sl = b->slots[b->next];
+    if (sl.pending)
+        cudaEventSynchronize(sl.done);
+    sl.pending = false;
     // workspaces come from each frame's filter pool and go back after the
     // launch: a mixed stream keeps them resident across batches instead of
     // reallocating whenever a slot's filter changes
@@ -203,48 +234,52 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
     }
     StagePlan plan;
     planStages(jobs, plan);
-    std::memcpy(b->hJobs, jobs.data(), sizeof(FrameJob) * count);
-    std::memcpy(b->hPrefix, plan.prefix.data(), plan.prefix.size() * sizeof(int));
+    std::memcpy(sl.hJobs, jobs.data(), sizeof(FrameJob) * count);
+    std::memcpy(sl.hPrefix, plan.prefix.data(), plan.prefix.size() * sizeof(int));
     int launches = -1;
     if (use_graph && !b->profiling) {
-        if (!b->exec || b->signature != sig) {
-            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        if (!sl.exec || sl.signature != sig) {
+            if (sl.exec) { cudaGraphExecDestroy(sl.exec); sl.exec = nullptr; }
+            sl.signature.clear();
             cudaGraph_t graph = nullptr;
             if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 giveBack();
                 return cudaFail(cudaGetLastError(), "graph capture");
             }
-            launches = enqueue(b, jobs, plan, s, true);
+            launches = enqueue(b, sl, jobs, plan, s);
             const cudaError_t e = cudaStreamEndCapture(s, &graph);
             if (e != cudaSuccess || launches < 0) {
+                if (graph) cudaGraphDestroy(graph);
                 giveBack();
                 return cudaFail(e != cudaSuccess ? e : cudaGetLastError(), "graph capture");
             }
-            const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+            const cudaError_t ie = cudaGraphInstantiate(&sl.exec, graph, 0);
             cudaGraphDestroy(graph);
             if (ie != cudaSuccess) {
+                sl.exec = nullptr;
                 giveBack();
                 return cudaFail(ie, "graph instantiate");
             }
-            b->signature = sig;
-            b->lastLaunches = launches;
+            sl.signature = sig;
+            sl.launches = launches;
         }
-        const cudaError_t e = cudaGraphLaunch(b->exec, s);
+        const cudaError_t e = cudaGraphLaunch(sl.exec, s);
         if (e != cudaSuccess) {
             giveBack();
             return cudaFail(e, "graph launch");
         }
-        launches = b->lastLaunches;
+        launches = sl.launches;
     } else {
-        launches = enqueue(b, jobs, plan, s, true);
+        launches = enqueue(b, sl, jobs, plan, s);
         if (launches < 0) {
             giveBack();
             return cudaFail(cudaGetLastError(), "lgcr_batch_run");
         }
-        b->lastLaunches = launches;
     }
-    cudaEventRecord(b->done, s);
-    b->pending = true;
+    b->lastLaunches = launches;
+    cudaEventRecord(sl.done, s);
+    sl.pending = true;
+    b->next = (b->next + 1) % kDescriptorSlots;
     for (Workspace *ws : taken) {
         cudaEventRecord(ws->done, s);
         ws->used = true;
