@@ -7,14 +7,19 @@ alternating algo 2 and algo 6, lanczos taps=4, sparse=1, qgate=1.0 -- on
 seeded synthetic polygon frames (seed = base + frame index, offset per rank).
 
   value        whole-job output-luma Mpix/s of the batched form (one launch per
-               stage over all 32 frames), inputs resident in HBM, CUDA events
-               on the launching stream, max over ranks
+               stage over all 32 frames, CUDA graph replay), inputs resident in
+               HBM, CUDA events on the launching stream, max over ranks
   e2e          same metric through the per-frame C ABI (lgcr_recon_frame) with
                pinned host planes: H2D, run, D2H inside the timed region, one
                calling host thread per core (at most 16) like fmParallel
   per_frame    device-resident per-frame path (one lgcr_recon_frame per frame)
-  roofline     dominant stage: algorithmic bytes (9 B per output pixel for
-               10-bit 4:2:0 -> 4:4:4) / its CUDA-event duration vs measured HBM
+  roofline     dominant stage: algorithmic bytes of the frames its launch
+               processes (9 B per output pixel for 10-bit 4:2:0 -> 4:4:4) / its
+               CUDA-event duration (separate event-bracketed pass) vs measured
+               HBM; for the guided stage also counted FP32 FLOPs vs nominal FP32
+  legs         the 1080p algo 2 batch (batched vs per-frame target) and the
+               plain 720p, jinc resize and bm+bp configurations: batched and
+               per-frame Mpix/s, stage split, roofline
   cpu_baseline the reference's AVX2 build on this host's cores (bounded sample)
   serving      the serving configuration's mixed stream (5 frame kinds, algo
                2/4/6, bm on 10 %, 24 streams) as Poisson arrivals at 1.2x the
@@ -30,7 +35,6 @@ import ctypes
 import json
 import multiprocessing as mp
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -127,19 +131,6 @@ class Clocks:
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": reasons, "samples": len(rows)}
-
-
-def read_traffic(stage):
-    """DRAM traffic per output pixel of one stage's kernel from the committed
-    ncu summary (line 'traffic_bytes_per_output_pixel <stage>: X'); the
-    caller scales it by the pixels of one launch. None when not captured."""
-    path = os.path.join(ROOT, "profiles", "recon_kernels_batched_8frames.md")
-    try:
-        m = re.search(r"traffic_bytes_per_output_pixel %s:\s*([0-9.eE+-]+)" % re.escape(stage),
-                      open(path).read())
-        return float(m.group(1)) if m else None
-    except Exception:
-        return None
 
 
 def measured_peaks():
@@ -377,17 +368,236 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+FORMATS = {"420P8": S.YUV420P8, "420P10": S.YUV420P10, "420P16": S.YUV420P16,
+           "420PS": S.YUV420PS, "422P10": S.YUV422P10, "444PS": S.YUV444PS}
+
+
+def leg_specs(rank: int):
+    """Frames of the timed legs beside the headline (each leg's frames are one
+    batch): the 1080p algo 2 batch the batched-vs-per-frame target is stated
+    on (the headline's 16 1080p frames, all run as algo 2), and the plain,
+    jinc-resize and block-refinement configurations."""
+    legs = {}
+    legs["north_star_1080p_algo2"] = dict(
+        reuse_headline=True, filter=dict(algo=2, **FILTER_ARGS),
+        workload="16x1920x1080 YUV420P10 -> 4:4:4, algo 2, lanczos taps=4, sparse=1, qgate=1.0")
+    legs["config0_720p_p8"] = dict(
+        frames=[dict(width=1280, height=720, fmt="420P8", seed=R.frame_seed(8000, rank, i), gen={})
+                for i in range(8)],
+        filter=dict(algo=2, kernel="lanczos", taps=3, strength=0.8, sigma=0.01),
+        workload="8x1280x720 YUV420P8 -> 4:4:4, algo 2, lanczos taps=3, strength 0.8, sigma 0.01")
+    for fmt, tag in (("420P16", "p16"), ("420PS", "ps")):
+        legs[f"config2_jinc_resize_{tag}"] = dict(
+            frames=[dict(width=1920, height=1080, fmt=fmt, seed=R.frame_seed(9000, rank, i),
+                         gen={"antialias": True}) for i in range(12)],
+            filter=dict(algo=4, kernel="jinc", taps=3, reg=0.005, width=3840, height=2160),
+            workload=f"12x1920x1080 YUV{fmt} -> 3840x2160 4:4:4, jinc taps=3, algo 4, reg 0.005")
+    legs["config3_bm_bp"] = dict(
+        frames=[dict(width=1920, height=1080, fmt="420P8", seed=R.frame_seed(10000, rank, i),
+                     gen={"extra_noise": True}) for i in range(16)],
+        filter=dict(algo=2, bm=1, bp=1.0),
+        workload="16x1920x1080 YUV420P8 (+noise) -> 4:4:4, algo 2, bm=1, bp=1.0")
+    return legs
+
+
+def _gen_any(task):
+    w, h, fmt, seed, gen = task
+    return S.make_frame(w, h, FORMATS[fmt], seed=seed, **gen)
+
+
+def generate_legs(legs, workers=None):
+    tasks, owners = [], []
+    for name, leg in legs.items():
+        for k, fr in enumerate(leg.get("frames", [])):
+            tasks.append((fr["width"], fr["height"], fr["fmt"], fr["seed"], fr["gen"]))
+            owners.append((name, k))
+    if not tasks:
+        return {}
+    workers = workers or min(len(tasks), max(1, (os.cpu_count() or 2) - 1), 16)
+    with mp.get_context("spawn").Pool(workers) as pool:
+        made = pool.map(_gen_any, tasks)
+    out = {}
+    for (name, k), planes in zip(owners, made):
+        out.setdefault(name, []).append(planes)
+    return out
+
+
+def algorithmic_bytes(planes, out_w, out_h):
+    """Compulsory HBM bytes of one frame: the input planes plus three output
+    planes at the output sample size."""
+    return sum(p.nbytes for p in planes) + 3 * out_w * out_h * planes[0].itemsize
+
+
+def stage_frames(stage, kinds):
+    """Indices of the frames a stage's launch processes; kinds[i] =
+    (algo, guided, bm, bp, resize)."""
+    def pick(fn):
+        return [i for i, k in enumerate(kinds) if fn(*k)]
+    if stage == "reconstructChroma":
+        return pick(lambda a, g, bm, bp, rs: g and a in (2, 4))
+    if stage.startswith(("buildAffineMaps", "buildDetail", "detailTransfer")):
+        return pick(lambda a, g, bm, bp, rs: g and a == 6)
+    if stage.startswith(("buildLGF", "blendSelector", "selector")):
+        return pick(lambda a, g, bm, bp, rs: g and a == 4)
+    if stage.startswith("collaborative"):
+        return pick(lambda a, g, bm, bp, rs: bm)
+    if stage.startswith("backProject"):
+        return pick(lambda a, g, bm, bp, rs: bp)
+    if stage.startswith("luma_resample"):
+        return pick(lambda a, g, bm, bp, rs: rs)
+    return list(range(len(kinds)))
+
+
+lgcr = None       # the package, imported after the frame generators' spawn pools
+
+
+class BatchLeg:
+    """Frames resident in HBM, their filters, and the batched / per-frame
+    device paths over them on one stream."""
+
+    def __init__(self, lib, dev, stream, filters, planes_list):
+        import numpy as np
+        import torch
+        self.lib, self.dev, self.stream = lib, dev, stream
+        self.filters = filters
+        self.dins, self.douts = [], []
+        tdt = {np.uint8: torch.uint8, np.uint16: torch.int16, np.float32: torch.float32}
+        for f, planes in zip(filters, planes_list):
+            ins = []
+            for p in planes:
+                t = torch.from_numpy(p.view(np.int16) if p.dtype == np.uint16 else p).to(dev)
+                ins.append(t.view(torch.uint16) if p.dtype == np.uint16 else t)
+            self.dins.append(ins)
+            odt = tdt[planes[0].dtype.type]
+            outs = [torch.empty((f.out_h, f.out_w), dtype=odt, device=dev) for _ in range(3)]
+            self.douts.append([o.view(torch.uint16) if odt == torch.int16 else o for o in outs])
+        self.items = (lgcr.BatchItem * len(filters))()
+        for i, f in enumerate(filters):
+            self.items[i].filter = f.handle
+            self.items[i].inp = lgcr.planes_desc(self.dins[i])
+            self.items[i].out = lgcr.planes_desc(self.douts[i])
+            self.items[i].chroma_location = -1
+        self.batch = ctypes.c_void_p()
+        assert lib.lgcr_batch_create(ctypes.byref(self.batch)) == 0
+        self.out_pixels = sum(f.out_w * f.out_h for f in filters)
+        self.algo_bytes = [algorithmic_bytes(p, f.out_w, f.out_h) for f, p in zip(filters, planes_list)]
+        self.in_bytes = sum(sum(p.nbytes for p in planes) for planes in planes_list)
+
+    def run(self, use_graph=1):
+        st = self.lib.lgcr_batch_run(self.batch, self.items, len(self.filters),
+                                     ctypes.c_void_p(self.stream.cuda_stream), use_graph)
+        if st != 0:
+            raise RuntimeError(self.lib.lgcr_last_error().decode())
+
+    def timed(self, fn, steps):
+        import torch
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(self.stream)
+        for _ in range(steps):
+            fn()
+        b.record(self.stream)
+        torch.cuda.synchronize(self.dev)
+        return a.elapsed_time(b)
+
+    def per_frame(self):
+        for i, f in enumerate(self.filters):
+            f.frame(self.dins[i], -1, out=self.douts[i], stream=self.stream.cuda_stream)
+
+    def stage_split(self, steps):
+        """Per-stage device ms per step from event-bracketed runs (a separate
+        pass: the bracketing bypasses the graph)."""
+        lib = self.lib
+        n = lib.lgcr_stage_count()
+        lib.lgcr_batch_set_profiling(self.batch, 1)
+        self.run(0)
+        lib.lgcr_batch_stage_times(self.batch, None, None, 1)
+        for _ in range(steps):
+            self.run(0)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int * n)()
+        lib.lgcr_batch_stage_times(self.batch, ms, cnt, 1)
+        lib.lgcr_batch_set_profiling(self.batch, 0)
+        return {lib.lgcr_stage_name(i).decode(): ms[i] / steps for i in range(n) if cnt[i]}
+
+    def sparse_active(self):
+        """Sparse-active ratio (trust-mask coverage) and active guided output
+        pixels per frame, from one untimed per-frame pass with stats."""
+        ratios, active = [], []
+        for i, f in enumerate(self.filters):
+            _, st = f.frame(self.dins[i], -1, out=self.douts[i], stream=self.stream.cuda_stream,
+                            stats=True)
+            ratios.append(st.sparse_active_ratio)
+            active.append(int(st.active_output_pixels))
+        return ratios, active
+
+    def close(self):
+        self.lib.lgcr_batch_destroy(self.batch)
+
+
+def axis_active_means(f):
+    """Mean active taps per output column and per output row of a filter's
+    chroma axes (the reference's tap metric counts activeX * activeY per
+    guided pixel, recon.cpp:253-257)."""
+    import numpy as np
+    lib = lgcr.library()
+    lib.lgcr_debug_axis.restype = ctypes.c_int
+    means = []
+    for axis, n in ((0, f.out_w), (1, f.out_h)):
+        shift = ctypes.c_double(-0.5 if axis == 0 else 0.0)
+        sup = ctypes.c_int()
+        lib.lgcr_debug_axis(f.handle, axis, shift, None, None, None, None, None, None, None,
+                            None, None, ctypes.byref(sup))
+        am = np.zeros(n * sup.value, np.uint8)
+        lib.lgcr_debug_axis(f.handle, axis, shift, None, None, am.ctypes.data_as(ctypes.c_void_p),
+                            None, None, None, None, None, None, ctypes.byref(sup))
+        means.append(float(am.reshape(n, sup.value).sum(1).mean()))
+    return means
+
+
+# FP32 arithmetic of one guided tap (tapsSeparable in kernels_recon.cu): 27
+# FP32 FLOPs (an FMA counted as 2) and 2 reciprocal approximations.
+GUIDED_FP32_FLOP_PER_TAP = 27
+FP32_LANES_PER_SM, B200_SMS = 128, 148
+
+
+def roofline_of(stage_ms, kinds, algo_bytes, peaks, steps_note):
+    """Dominant stage: achieved algorithmic GB/s over the frames its launch
+    processes vs the measured HBM copy bandwidth."""
+    if not stage_ms:
+        return None
+    dominant = max(stage_ms, key=stage_ms.get)
+    frames = stage_frames(dominant, kinds)
+    launch_ms = stage_ms[dominant]
+    nbytes = sum(algo_bytes[i] for i in frames)
+    achieved = nbytes / (launch_ms / 1000.0) / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    step_ms = sum(stage_ms.values())
+    return {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "launch_ms": round(launch_ms, 3), "frames_in_launch": len(frames),
+            "algorithmic_bytes_per_launch": int(nbytes),
+            "step_hbm_frac": round(sum(algo_bytes) / (step_ms / 1000.0) / 1e9 / peak, 4),
+            "stage_ms_per_step": {k: round(v, 3) for k, v in
+                                  sorted(stage_ms.items(), key=lambda kv: -kv[1])},
+            "stage_timing": steps_note}
+
+
 def our_arm(args):
+    global lgcr
     rank, world, local = R.rank_info()
     specs = frame_specs(rank, args.frames)
-    frames = generate(specs)                      # before CUDA init (spawn pool)
+    frames = generate(specs)                      # before CUDA init (spawn pools)
+    legs = leg_specs(rank) if not args.no_legs else {}
+    leg_frames = generate_legs(legs)
     cpu_frames = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_frames = frames
 
     import numpy as np
     import torch
-    import lgcr
+    import lgcr as _lgcr
+    lgcr = _lgcr
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
@@ -399,115 +609,77 @@ def our_arm(args):
     lib.lgcr_batch_stage_times.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.lgcr_stage_name.restype = ctypes.c_char_p
-    nstages = lib.lgcr_stage_count()
-
-    # filters (one per geometry x algo) and device-resident frames
-    filt = {}
-    for spec in specs:
-        key = (spec["width"], spec["height"], spec["algo"])
-        if key not in filt:
-            fmt = lgcr.video_format(spec["width"], spec["height"], 10, 1, 1)
-            filt[key] = lgcr.Recon(fmt, algo=spec["algo"], **FILTER_ARGS)
-    dins, douts = [], []
-    for spec, planes in zip(specs, frames):
-        dins.append([torch.from_numpy(p.astype(np.int16, copy=False).view(np.int16)).to(dev)
-                     .view(torch.uint16) for p in planes])
-        douts.append([torch.empty((spec["height"], spec["width"]), dtype=torch.uint16, device=dev)
-                      for _ in range(3)])
-    items = (lgcr.BatchItem * len(specs))()
-    for i, spec in enumerate(specs):
-        items[i].filter = filt[(spec["width"], spec["height"], spec["algo"])].handle
-        items[i].inp = lgcr.planes_desc(dins[i])
-        items[i].out = lgcr.planes_desc(douts[i])
-        items[i].chroma_location = -1
-    batch = ctypes.c_void_p()
-    assert lib.lgcr_batch_create(ctypes.byref(batch)) == 0
+    peaks = measured_peaks()
     stream = torch.cuda.Stream(device=dev)
-    sh = stream.cuda_stream
-    out_pixels = sum(s["width"] * s["height"] for s in specs)
-    in_bytes = sum(sum(p.nbytes for p in f) for f in frames)
-
-    def run_batch(use_graph=0):
-        st = lib.lgcr_batch_run(batch, items, len(specs), ctypes.c_void_p(sh), use_graph)
-        if st != 0:
-            raise RuntimeError(lib.lgcr_last_error().decode())
 
     def barrier():
         torch.cuda.synchronize(dev)
         if world > 1:
             torch.distributed.barrier()
 
+    # filters (one per geometry x algo) and the headline batch, resident in HBM
+    filt = {}
+    for spec in specs:
+        key = (spec["width"], spec["height"], spec["algo"])
+        if key not in filt:
+            fmt = lgcr.video_format(spec["width"], spec["height"], 10, 1, 1)
+            filt[key] = lgcr.Recon(fmt, algo=spec["algo"], **FILTER_ARGS)
+    head_filters = [filt[(s["width"], s["height"], s["algo"])] for s in specs]
+    head = BatchLeg(lib, dev, stream, head_filters, frames)
+    out_pixels = head.out_pixels
+
     # autotune launch shapes / register budget on this workload (untimed)
     tuned = ""
     if not args.no_autotune:
         rep = ctypes.create_string_buffer(4096)
-        if lib.lgcr_autotune(items, len(specs), ctypes.c_void_p(sh), rep, 4096) == 0:
+        if lib.lgcr_autotune(head.items, len(specs), ctypes.c_void_p(stream.cuda_stream), rep, 4096) == 0:
             tuned = rep.value.decode()
         torch.cuda.synchronize(dev)
 
-    # warm-up (also builds tables, workspaces, the graph)
-    lib.lgcr_batch_set_profiling(batch, 1)
+    # warm-up (tables, workspaces, the graphs of this layout)
     for _ in range(max(args.warmup, 1)):
-        run_batch()
+        head.run(1)
     barrier()
-    lib.lgcr_batch_stage_times(batch, None, None, 1)
 
-    # timed region: batched form, per-stage events on the launching stream
+    # timed region: batched form, graph replay, stage profiling off
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
         barrier()
         start.record(stream)
         for _ in range(args.steps):
-            run_batch()
+            head.run(1)
         stop.record(stream)
         barrier()
     elapsed_ms = start.elapsed_time(stop)
-    launches_per_step = lib.lgcr_batch_launch_count(batch)
-    ms_arr = (ctypes.c_double * nstages)()
-    cnt_arr = (ctypes.c_int * nstages)()
-    lib.lgcr_batch_stage_times(batch, ms_arr, cnt_arr, 1)
-    stage_ms = {lib.lgcr_stage_name(i).decode(): ms_arr[i] for i in range(nstages) if cnt_arr[i]}
+    launches_per_step = lib.lgcr_batch_launch_count(head.batch)
     max_ms = R.max_over_ranks(elapsed_ms, dev)
     value = out_pixels * world * args.steps / (max_ms / 1000.0) / 1e6
+    clocks = clk.summary()
 
-    lib.lgcr_batch_set_profiling(batch, 0)
+    # stage split from a separate event-bracketed pass (not the timed region)
+    prof_steps = max(2, min(args.steps, 5))
+    stage_ms = head.stage_split(prof_steps)
+    barrier()
     if args.batch_only:
-        lib.lgcr_batch_destroy(batch)
+        head.close()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": round(value, 2), "unit": "Mpix/s",
                               "frames_per_step": len(specs), "batch_only": True,
                               "ms_per_step": round(max_ms / args.steps, 3),
-                              "stage_ms_per_step": {k: round(v / max(1, args.steps), 3) for k, v in
+                              "stage_ms_per_step": {k: round(v, 3) for k, v in
                                                     sorted(stage_ms.items(), key=lambda kv: -kv[1])}}))
         if world > 1:
             torch.distributed.destroy_process_group()
         return 0
 
-    # graph replay of the same layout (reported, not the headline)
-    run_batch(1)
-    barrier()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(args.steps):
-        run_batch(1)
-    g1.record(stream)
-    barrier()
-    graph_ms = g0.elapsed_time(g1)
-
+    # direct launches (no graph) of the same batch, for comparison
+    head.run(0)
+    direct_ms = head.timed(lambda: head.run(0), args.steps)
     # per-frame device path: one lgcr_recon_frame per frame on one stream
-    def per_frame_pass():
-        for i, spec in enumerate(specs):
-            f = filt[(spec["width"], spec["height"], spec["algo"])]
-            f.frame(dins[i], -1, out=douts[i], stream=sh)
-    per_frame_pass()
+    head.per_frame()
+    per_frame_ms = head.timed(head.per_frame, args.steps)
     barrier()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    for _ in range(args.steps):
-        per_frame_pass()
-    p1.record(stream)
-    barrier()
-    per_frame_ms = p0.elapsed_time(p1)
+    ratios, active = head.sparse_active()
 
     # e2e: host planes in pinned memory through the per-frame C ABI, one host
     # thread per core (frame-parallel like the reference's fmParallel)
@@ -537,8 +709,7 @@ def our_arm(args):
                     if not queue:
                         return
                     i = queue.pop(0)
-                spec = specs[i]
-                f = filt[(spec["width"], spec["height"], spec["algo"])]
+                f = head_filters[i]
                 t0 = time.perf_counter()
                 f.frame(pinned_in[i], -1, out=pinned_out[i])
                 with lock:
@@ -565,23 +736,26 @@ def our_arm(args):
     e2e_value = out_pixels * world * args.steps / e2e_s / 1e6
     out_bytes_e2e = sum(2 * s["width"] * s["height"] * 2 for s in specs)   # U, V (luma shared)
 
-    # roofline of the dominant stage
-    peaks = measured_peaks()
-    dominant = max(stage_ms, key=stage_ms.get) if stage_ms else None
-    rl = None
-    if dominant:
-        per_launch_ms = stage_ms[dominant] / max(1, args.steps)
-        algo_bytes = BYTES_PER_PIXEL * out_pixels
-        achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
-        peak = peaks.get("hbm_gbs", 6650.0)
-        tpp = read_traffic(dominant)
-        rl = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
-              "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-              "traffic": (round(tpp * out_pixels) if tpp else None),
-              "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-              "launch_ms": round(per_launch_ms, 3),
-              "stage_ms_per_step": {k: round(v / max(1, args.steps), 3) for k, v in
-                                    sorted(stage_ms.items(), key=lambda kv: -kv[1])}}
+    # roofline of the dominant stage, with the guided stage's FP32 side
+    kinds = [(s["algo"], True, False, False, False) for s in specs]
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    rl = roofline_of(stage_ms, kinds, head.algo_bytes, peaks,
+                     f"event-bracketed pass of {prof_steps} steps")
+    if rl and rl["kernel"] == "reconstructChroma":
+        mx, my = axis_active_means(head_filters[0])
+        guided = stage_frames("reconstructChroma", kinds)
+        taps = sum(active[i] for i in guided) * mx * my
+        flops = taps * GUIDED_FP32_FLOP_PER_TAP
+        fp32_peak = B200_SMS * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+        achieved_tf = flops / (rl["launch_ms"] / 1000.0) / 1e12
+        rl["binding_bound"] = ("instruction issue of the FP32 (packed pairs), FP64 "
+                               "accumulation and reciprocal pipes")
+        rl["fp32"] = {"achieved_tflops": round(achieved_tf, 2), "peak_tflops": round(fp32_peak, 1),
+                      "frac": round(achieved_tf / fp32_peak, 4),
+                      "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 FLOP x sampled SM clock",
+                      "taps_per_step": int(taps),
+                      "taps_source": "active guided pixels x mean active taps per column x per row",
+                      "flop_per_tap": GUIDED_FP32_FLOP_PER_TAP}
 
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
@@ -593,22 +767,66 @@ def our_arm(args):
                    "output_mpix_per_step": round(out_pixels / 1e6, 3),
                    "l2": "inputs larger than L2: ~250 MB in + 1 GB out per step",
                    "accumulation": "f32 with f64 accumulators (as the reference)",
+                   "path": "batched form, CUDA graph replay, stage profiling off",
                    "parallelism": f"replicas x{world}",
                    "autotune": [l for l in tuned.splitlines() if l]},
+        "sparse_active_ratio": {"mean": round(float(np.mean(ratios)), 4),
+                                "min": round(float(np.min(ratios)), 4),
+                                "max": round(float(np.max(ratios)), 4)},
         "per_frame": {"value": round(out_pixels * args.steps / (per_frame_ms / 1000) / 1e6, 2),
                       "unit": "Mpix/s", "ms_per_step": round(per_frame_ms / args.steps, 3)},
-        "graph_replay": {"value": round(out_pixels * args.steps / (graph_ms / 1000) / 1e6, 2),
-                         "unit": "Mpix/s", "ms_per_step": round(graph_ms / args.steps, 3)},
+        "direct_launches": {"value": round(out_pixels * args.steps / (direct_ms / 1000) / 1e6, 2),
+                            "unit": "Mpix/s", "ms_per_step": round(direct_ms / args.steps, 3)},
         "batched_vs_per_frame": round(per_frame_ms / max(elapsed_ms, 1e-9), 3),
         "latency_ms": {"p50": round(statistics.median(latencies), 3) if latencies else None,
                        "p99": round(sorted(latencies)[int(0.99 * (len(latencies) - 1))], 3)
                        if latencies else None, "per": "frame, e2e host path"},
         "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "host_threads": e2e_threads,
-                "h2d_bytes_per_step": int(in_bytes), "d2h_bytes_per_step": int(out_bytes_e2e)},
+                "h2d_bytes_per_step": int(head.in_bytes), "d2h_bytes_per_step": int(out_bytes_e2e)},
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": rl,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
+    head.close()
+
+    # the other legs: batched (graph) vs per-frame, stage split, roofline
+    if legs:
+        out_legs = {}
+        leg_steps = max(3, min(args.steps, 10))
+        for name, leg in legs.items():
+            if leg.get("reuse_headline"):
+                planes_list = [frames[i] for i, s in enumerate(specs) if s["width"] == 1920]
+            else:
+                planes_list = leg_frames[name]
+            lf = [lgcr.Recon(lgcr.format_of(p, 10 if leg.get("reuse_headline") else None),
+                             **leg["filter"]) for p in planes_list]
+            b = BatchLeg(lib, dev, stream, lf, planes_list)
+            for _ in range(max(args.warmup, 1)):
+                b.run(1)
+            barrier()
+            bms = b.timed(lambda: b.run(1), leg_steps)
+            b.per_frame()
+            pms = b.timed(b.per_frame, leg_steps)
+            sms = b.stage_split(2)
+            lr, _ = b.sparse_active()
+            fa = leg["filter"]
+            kinds = [(fa.get("algo", 2), fa.get("strength", 0.8) > 0, bool(fa.get("bm")),
+                      fa.get("bp", 0.0) > 0, "width" in fa)] * len(lf)
+            out_legs[name] = {
+                "workload": leg["workload"], "frames": len(lf),
+                "batched": {"value": round(b.out_pixels * leg_steps / (bms / 1000) / 1e6, 2),
+                            "unit": "Mpix/s", "ms_per_step": round(bms / leg_steps, 3)},
+                "per_frame": {"value": round(b.out_pixels * leg_steps / (pms / 1000) / 1e6, 2),
+                              "unit": "Mpix/s", "ms_per_step": round(pms / leg_steps, 3)},
+                "batched_vs_per_frame": round(pms / max(bms, 1e-9), 3),
+                "sparse_active_ratio": round(float(np.mean(lr)), 4),
+                "launches_per_step": lib.lgcr_batch_launch_count(b.batch),
+                "roofline": roofline_of(sms, kinds, b.algo_bytes, peaks,
+                                        "event-bracketed pass of 2 steps")}
+            b.close()
+            del lf
+        result["legs"] = out_legs
+
     if rank == 0 and args.serve_requests > 0:
         # content of the serving stream (spawned workers: safe after CUDA init)
         keys = [(k, s) for k in range(len(SERVE_KINDS)) for s in range(SERVE_SEEDS)]
@@ -624,7 +842,6 @@ def our_arm(args):
             "sample": f"{len(times)} rounds of {threads} frames (alternating 1080p/4K, algo 2/6, "
                       f"one frame per thread) from the workload, reference AVX2 build "
                       f"(oracle/_ref), {total_s:.1f} s"}
-    lib.lgcr_batch_destroy(batch)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -652,7 +869,12 @@ def main():
                     help="concurrent device batches of the serving leg")
     ap.add_argument("--batch-only", action="store_true",
                     help="time the batched form only (profiler captures)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the north-star and per-configuration legs")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the replicas under torchrun
+        return R.relaunch(os.path.abspath(__file__), sys.argv[1:], args.gpus)
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

@@ -1,6 +1,6 @@
 """CPU checks of bench.py's pure helpers: the workload it times, the CPU
-baseline's sample order, and the roofline traffic it reads from the committed
-ncu summary."""
+baseline's sample order, the frames each stage's roofline is charged with,
+and the legs beside the headline."""
 import os
 import sys
 
@@ -42,8 +42,32 @@ def test_cpu_sample_alternates_sizes():
     assert all(widths[k] != widths[k + 1] for k in range(31))
 
 
-def test_roofline_traffic_per_stage():
-    for stage in ("plainChroma", "reconstructChroma"):
-        t = bench.read_traffic(stage)
-        assert t is not None and 1.0 < t < 100.0, stage
-    assert bench.read_traffic("no_such_stage") is None
+def test_roofline_attributes_each_stage_to_its_frames():
+    # (algo, guided, bm, bp, resize) per frame: the headline alternates 2 and 6
+    kinds = [(s["algo"], True, False, False, False) for s in bench.frame_specs(0)]
+    guided = bench.stage_frames("reconstructChroma", kinds)
+    assert len(guided) == 16 and all(kinds[i][0] == 2 for i in guided)
+    assert len(bench.stage_frames("buildAffineMaps_listed", kinds)) == 16
+    assert len(bench.stage_frames("plainChroma", kinds)) == 32
+    stage_ms = {"reconstructChroma": 4.0, "plainChroma": 3.0}
+    algo_bytes = [9 * s["width"] * s["height"] for s in bench.frame_specs(0)]
+    rl = bench.roofline_of(stage_ms, kinds, algo_bytes, {"hbm_gbs": 6500.0}, "test")
+    assert rl["kernel"] == "reconstructChroma" and rl["frames_in_launch"] == 16
+    assert rl["algorithmic_bytes_per_launch"] == sum(algo_bytes[i] for i in guided)
+    assert abs(rl["frac"] - rl["achieved"] / 6500.0) < 1e-3
+    assert rl["traffic"] is None
+
+
+def test_algorithmic_bytes_match_the_formula():
+    import numpy as np
+    planes = (np.zeros((1080, 1920), np.uint16), np.zeros((540, 960), np.uint16),
+              np.zeros((540, 960), np.uint16))
+    assert bench.algorithmic_bytes(planes, 1920, 1080) == 9 * 1920 * 1080
+
+
+def test_legs_cover_the_other_configurations():
+    legs = bench.leg_specs(0)
+    assert set(legs) == {"north_star_1080p_algo2", "config0_720p_p8", "config2_jinc_resize_p16",
+                         "config2_jinc_resize_ps", "config3_bm_bp"}
+    assert len(legs["config2_jinc_resize_p16"]["frames"]) == 12
+    assert legs["config3_bm_bp"]["filter"]["bm"] == 1

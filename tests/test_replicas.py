@@ -49,3 +49,13 @@ def test_max_over_ranks_gloo_world2():
         assert out[r][0] == 11.0             # max over ranks
         assert out[r][1] == 10.0             # shards cover all frames
     assert R.aggregate_throughput([100, 100], 2.0) == 100.0
+
+
+def test_relaunch_starts_one_process_per_replica(capfd):
+    import json
+    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "replica_child.py")
+    assert R.launch_command(child, ["--x"], 2, 1234)[-2:] == [child, "--x"]
+    rc = R.relaunch(child, [], 2, timeout_s=300)
+    assert rc == 0
+    line = [l for l in capfd.readouterr().out.splitlines() if l.startswith("{")][-1]
+    assert json.loads(line) == {"world": 2, "max": 11.0, "frames": 32.0}

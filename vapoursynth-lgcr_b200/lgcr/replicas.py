@@ -8,6 +8,9 @@ the only cross-rank step is the max over ranks of the measured time.
 from __future__ import annotations
 
 import os
+import socket
+import subprocess
+import sys
 
 
 def rank_info():
@@ -42,3 +45,28 @@ def max_over_ranks(value: float, device=None) -> float:
 def aggregate_throughput(units_per_rank, seconds_max: float) -> float:
     """Whole-job throughput: units over all ranks / max-over-ranks time."""
     return float(sum(units_per_rank)) / seconds_max
+
+
+def free_port() -> int:
+    """An unused TCP port on the loopback interface."""
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def launch_command(script: str, argv, nproc: int, port: int):
+    """torchrun command that starts `nproc` replicas of `script` on this node
+    (one process per GPU), rendezvous on 127.0.0.1."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={int(nproc)}", "--master-addr", "127.0.0.1",
+            "--master-port", str(int(port)), script] + list(argv)
+
+
+def relaunch(script: str, argv, nproc: int, timeout_s: float = 3600.0) -> int:
+    """Run `script` as `nproc` replicas under torchrun and return its exit
+    status (used when a multi-GPU run is started without torchrun)."""
+    cmd = launch_command(script, argv, nproc, free_port())
+    try:
+        return subprocess.run(cmd, timeout=timeout_s).returncode
+    except subprocess.TimeoutExpired:
+        return 124
