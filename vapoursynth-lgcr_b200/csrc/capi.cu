@@ -11,9 +11,11 @@ namespace lgcr_b200 {
 const char *lastError();
 }
 
-namespace {
+namespace lgcr_b200 {
 
-int *zeroPrefix() {
+// Stage prefix table of a single-frame launch (every stage starts at block
+// 0): zeros, shared by all single-frame calls.
+const int *singleFramePrefix() {
     static int *buf = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -23,12 +25,18 @@ int *zeroPrefix() {
     return buf;
 }
 
-cudaStream_t threadStream() {
+// The calling host thread's own non-blocking stream (host-memory calls
+// without a caller stream).
+cudaStream_t callingThreadStream() {
     thread_local cudaStream_t s = nullptr;
     if (!s)
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     return s;
 }
+
+} // namespace lgcr_b200
+
+namespace {
 
 // Completion event of the calling thread's frames (blocking sync), or null.
 cudaEvent_t threadDoneEvent() {
@@ -123,7 +131,7 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         setError("LGCR: memory must be LGCR_MEM_HOST or LGCR_MEM_DEVICE");
         return LGCR_E_ARGUMENT;
     }
-    cudaStream_t s = stream ? (cudaStream_t)stream : (memory == LGCR_MEM_HOST ? threadStream() : nullptr);
+    cudaStream_t s = stream ? (cudaStream_t)stream : (memory == LGCR_MEM_HOST ? callingThreadStream() : nullptr);
     FrameTask t;
     t.filter = &F;
     t.p = F.sited(chroma_location);
@@ -167,7 +175,7 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         std::vector<FrameJob> jobs(1, *ws->hJob);
         StagePlan plan;
         planStages(jobs, plan);
-        if (launchStages(jobs, plan, ws->dJob, zeroPrefix(), s) < 0)
+        if (launchStages(jobs, plan, ws->dJob, singleFramePrefix(), s) < 0)
             e = cudaGetLastError();
     }
     if (e == cudaSuccess && memory == LGCR_MEM_HOST) {

@@ -193,6 +193,11 @@ inline cudaError_t copyPlane(void *dst, size_t dpitch, const void *src, size_t s
 }
 int cudaFail(cudaError_t e, const char *where);
 
+// Zero stage prefix table for single-frame launches (device memory).
+const int *singleFramePrefix();
+// The calling host thread's own non-blocking stream.
+cudaStream_t callingThreadStream();
+
 } // namespace lgcr_b200
 
 // Handle type of the C ABI.
