@@ -13,6 +13,10 @@
  *   lgcr_recon_frame       <- lgcrGetFrame          src/plugin.cpp:177-721
  *   lgcr_batch_*           <- frame-parallel getFrame calls (fmParallel,
  *                             src/plugin.cpp:1157) folded into one launch
+ *   lgcr_sharpen_*         <- sharpenCreate / sharpenGetFrame / sharpenFree
+ *                             src/plugin.cpp:14-111
+ *   lgcr_trecon_*          <- tReconCreate / tReconGetFrame
+ *                             src/plugin.cpp:723-990
  *   lgcr_server_*          <- the VapourSynth core's concurrent request
  *                             scheduling of Recon frames (no single
  *                             reference symbol; see plugin.cpp:215-217
@@ -188,6 +192,86 @@ int lgcr_debug_axis(const lgcr_recon *filter, int axis, double shift, int *start
  * differing results to *mismatches (0 expected). No counterpart in the
  * reference (its divides are plain C++). */
 int lgcr_selftest_reciprocal(uint64_t *mismatches);
+
+/* ---------------------------------------------------------------------
+ * Sharpen: the reference's second filter, a 5x5 gated bilateral unsharp
+ * mask (luma self-guided; subsampled chroma guided by the sharpened luma's
+ * footprint map; 4:4:4 chroma self-guided). Same format in and out.
+ *   lgcr_sharpen_create   <- sharpenCreate    src/plugin.cpp:84-111
+ *   lgcr_sharpen_frame    <- sharpenGetFrame  src/plugin.cpp:14-76
+ *   lgcr_sharpen_destroy  <- sharpenFree      src/plugin.cpp:78-82
+ * ------------------------------------------------------------------- */
+/* Sharpen arguments, one field per entry of the reference signature
+ *   clip:vnode;alpha:float:opt;sigma:float:opt;sratio:float:opt;
+ *   gspatial:float:opt;ar:float:opt          (src/plugin.cpp:1172-1176)
+ * NaN = not given (defaults 0.3, 0.01, 0.15, 1.2, 0.0). */
+typedef struct lgcr_sharpen_params {
+    double alpha, sigma, sratio, gspatial, ar;
+} lgcr_sharpen_params;
+
+typedef struct lgcr_sharpen lgcr_sharpen;
+
+void lgcr_sharpen_params_init(lgcr_sharpen_params *params);
+/* Validates like sharpenCreate and returns LGCR_E_INVALID with its message
+ * ("LGCR Sharpen: planar YUV only", "LGCR Sharpen: sigma/sratio/gspatial
+ * must be > 0"). fmt->width/height 0 accepts any frame size. */
+int lgcr_sharpen_create(const lgcr_sharpen_params *params, const lgcr_format *fmt,
+                        lgcr_sharpen **out, char *err, size_t errlen);
+void lgcr_sharpen_destroy(lgcr_sharpen *filter);
+/* One frame: in/out Y, U, V planes of the clip's format (all three output
+ * planes are written). memory as for lgcr_recon_frame: LGCR_MEM_HOST
+ * uploads, runs, downloads and returns when done; LGCR_MEM_DEVICE enqueues
+ * on `stream` without waiting. Safe to call from several host threads. */
+int lgcr_sharpen_frame(lgcr_sharpen *filter, const lgcr_plane in[3], const lgcr_plane out[3],
+                       int memory, void *stream);
+
+/* ---------------------------------------------------------------------
+ * TRecon: motion-compensated temporal Recon (same-size 4:2:0/4:2:2/4:4:4
+ * -> 4:4:4, lanczos3 base, algo 2). Each frame is reconstructed with the
+ * chroma samples of its temporal neighbours as extra taps, after 16x16
+ * block matching on luma and a chroma-consistency check per block.
+ *   lgcr_trecon_create    <- tReconCreate     src/plugin.cpp:920-990
+ *   lgcr_trecon_neighbors <- temporalFrameNumbers src/plugin.cpp:729-738
+ *   lgcr_trecon_frame     <- tReconGetFrame   src/plugin.cpp:740-918
+ *   lgcr_trecon_destroy   <- lgcrFree         src/plugin.cpp:992-996
+ * ------------------------------------------------------------------- */
+/* TRecon arguments, one field per entry of the reference signature
+ *   clip:vnode;strength:float:opt;sigma:float:opt;sratio:float:opt;
+ *   sdb:float:opt;gsigma:float:opt;stretch:float:opt;ar:float:opt;
+ *   ridge:int:opt;sparse:int:opt;ms:float:opt;trad:int:opt;
+ *   tsearch:int:opt;tsad:float:opt;bm:int:opt  (src/plugin.cpp:1177-1181)
+ * Doubles NaN and ints LGCR_UNSET_INT mean "not given". */
+typedef struct lgcr_trecon_params {
+    double strength, sigma, sratio, sdb, gsigma, stretch, ar;
+    int ridge, sparse;
+    double ms;
+    int trad, tsearch;
+    double tsad;
+    int bm;
+} lgcr_trecon_params;
+
+typedef struct lgcr_trecon lgcr_trecon;
+
+void lgcr_trecon_params_init(lgcr_trecon_params *params);
+/* Validates like tReconCreate (the clip's frame count is num_frames) and
+ * returns LGCR_E_INVALID with its message on failure. */
+int lgcr_trecon_create(const lgcr_trecon_params *params, const lgcr_format *fmt,
+                       int num_frames, lgcr_trecon **out, char *err, size_t errlen);
+void lgcr_trecon_destroy(lgcr_trecon *filter);
+/* Frame numbers frame n needs besides itself, in the order
+ * lgcr_trecon_frame expects them (n +- trad clamped to the clip, without n,
+ * without repeats). Returns their count (at most 2 * trad); frames holds up
+ * to cap of them. */
+int lgcr_trecon_neighbors(const lgcr_trecon *filter, int n, int *frames, int cap);
+/*
+ * One frame: cur[0..2] the frame's Y, U, V; nbrs[3*k .. 3*k+2] the planes of
+ * the k-th neighbour from lgcr_trecon_neighbors (count of them; ignored when
+ * strength is 0); out[0..2] 4:4:4 Y, U, V (all written). chroma_location,
+ * memory and stream as for lgcr_recon_frame.
+ */
+int lgcr_trecon_frame(lgcr_trecon *filter, const lgcr_plane cur[3], const lgcr_plane *nbrs,
+                      int count, const lgcr_plane out[3], int chroma_location, int memory,
+                      void *stream);
 
 /* ---------------------------------------------------------------------
  * Batched form: many frames (any mix of filters, sizes, subsamplings and

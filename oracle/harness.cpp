@@ -1,15 +1,19 @@
 // oracle/harness.cpp — TEST INFRASTRUCTURE ONLY (the oracle).
 //
-// Restates the per-frame orchestration of the reference's Recon filter over
-// raw planar host buffers, so that the reference's own compute functions
-// (compiled unmodified from src/{maps,kernels,recon,algos,bm,workspace,
-// pipeline}.cpp of MysteryDove/vapoursynth-LGCR) can be driven without
-// VapourSynth. Only tests, the smoke check and the bench's CPU-baseline leg
+// Restates the per-frame orchestration of the reference's Recon, Sharpen and
+// TRecon filters over raw planar host buffers, so that the reference's own
+// compute functions (compiled unmodified from src/{maps,kernels,recon,algos,
+// bm,workspace,pipeline}.cpp of MysteryDove/vapoursynth-LGCR) can be driven
+// without VapourSynth. Only tests, the smoke check and the bench's CPU-baseline leg
 // load the library built from this file; the product never does.
 //
 //   oracle_create  restates lgcrCreate          src/plugin.cpp:998-1158
 //   oracle_frame   restates lgcrGetFrame        src/plugin.cpp:177-721
 //                  with applyFrameChromaSiting  src/plugin.cpp:157-175
+//   oracle_sharpen_frame restates sharpenCreate + sharpenGetFrame
+//                                               src/plugin.cpp:14-111
+//   oracle_trecon_frame  restates tReconCreate + tReconGetFrame
+//                                               src/plugin.cpp:723-990
 // VapourSynth calls are replaced by plane pointers; the numeric path is the
 // reference's, function for function.
 #include "lgcr.h"
@@ -649,3 +653,247 @@ int oracle_jinc_lut(void *handle, oracle_f32 *lut, int *n) {
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Sharpen (plugin.cpp:14-111): sharpenCreate's argument defaults and checks,
+// then sharpenGetFrame's sequence over raw planes, calling the reference's
+// planeToFloat, sharpenPlane (algos.cpp:595-659), buildGuideMaps and
+// floatToPlane.
+// ---------------------------------------------------------------------------
+namespace {
+
+void extractPlanes(const lgcr_plane *in, const lgcr_format &fmt, Plane &y, Plane &cb, Plane &cr,
+                   bool chromaOffset) {
+    const bool isFloat = fmt.sample_type == LGCR_ST_FLOAT;
+    const int bytes = isFloat ? 4 : (fmt.bits_per_sample > 8 ? 2 : 1);
+    const double yScale = isFloat ? 1.0 : 1.0 / double((1 << fmt.bits_per_sample) - 1);
+    Plane *dst[3] = { &y, &cb, &cr };
+    for (int p = 0; p < 3; ++p) {
+        const uint8_t *src = static_cast<const uint8_t *>(in[p].data);
+        const double off = (p == 0 || isFloat || !chromaOffset) ? 0.0 : -0.5;
+        if (isFloat) {
+            // planeToFloat<float>(.., 1.0, 0.0): s * 1.0 + 0.0 in double
+            for (int row = 0; row < dst[p]->h; ++row) {
+                const oracle_f32 *s = reinterpret_cast<const oracle_f32 *>(src + in[p].stride * row);
+                for (int x = 0; x < dst[p]->w; ++x)
+                    dst[p]->row(row)[x] = static_cast<oracle_f32>(s[x] * 1.0 + 0.0);
+            }
+        } else if (bytes == 1) {
+            planeToFloat<uint8_t>(src, in[p].stride, *dst[p], dst[p]->w, dst[p]->h, yScale, off);
+        } else {
+            planeToFloat<uint16_t>(src, in[p].stride, *dst[p], dst[p]->w, dst[p]->h, yScale, off);
+        }
+    }
+}
+
+void storeOutputPlane(const Plane &s, const lgcr_plane &out, const lgcr_format &fmt, bool chroma) {
+    const bool isFloat = fmt.sample_type == LGCR_ST_FLOAT;
+    const int bytes = isFloat ? 4 : (fmt.bits_per_sample > 8 ? 2 : 1);
+    const double outScale = isFloat ? 1.0 : double((1 << fmt.bits_per_sample) - 1);
+    const double outOff = (!chroma || isFloat) ? 0.0 : 0.5 * outScale;
+    if (isFloat)
+        storeFloatPlane(s, out);
+    else if (bytes == 1)
+        storePlane<uint8_t>(s, out, outScale, outOff, 0, 255);
+    else
+        storePlane<uint16_t>(s, out, outScale, outOff, 0,
+                             uint16_t((1 << fmt.bits_per_sample) - 1));
+}
+
+} // namespace
+
+extern "C" int oracle_sharpen_frame(const lgcr_format *fmt, double alpha, double sigma,
+                                    double sratio, double gspatial, double ar,
+                                    const lgcr_plane *in, const lgcr_plane *out, char *err,
+                                    size_t errlen) {
+    if (fmt->color_family != LGCR_CF_YUV ||
+        (fmt->sample_type == LGCR_ST_FLOAT && fmt->bits_per_sample != 32)) {
+        copyError(err, errlen, "LGCR Sharpen: planar YUV only");
+        return LGCR_E_INVALID;
+    }
+    SharpenData d;
+    if (given(alpha)) d.alpha = alpha;
+    if (given(sigma)) d.sigma = sigma;
+    if (given(sratio)) d.sratio = sratio;
+    if (given(gspatial)) d.gspatial = gspatial;
+    if (given(ar)) d.arMargin = ar;
+    if (d.sigma <= 0.0 || d.sratio <= 0.0 || d.gspatial <= 0.0) {
+        copyError(err, errlen, "LGCR Sharpen: sigma/sratio/gspatial must be > 0");
+        return LGCR_E_INVALID;
+    }
+    const int sw = in[0].width, sh = in[0].height, cw = in[1].width, ch = in[1].height;
+    Plane y(sw, sh), cb(cw, ch), cr(cw, ch);
+    extractPlanes(in, *fmt, y, cb, cr, true);
+    sharpenPlane(y, nullptr, y, 1.0, 1.0, 0.0, 0.0, d);
+    if (cw != sw || ch != sh) {
+        const double rw = double(sw) / cw, rh = double(sh) / ch;
+        GuideMaps gm = buildGuideMaps(y, y, cw, ch, rw, rh, -0.5, 0.0);
+        sharpenPlane(cb, &gm.lc, y, rw, rh, -0.5, 0.0, d);
+        sharpenPlane(cr, &gm.lc, y, rw, rh, -0.5, 0.0, d);
+    } else {
+        sharpenPlane(cb, nullptr, cb, 1.0, 1.0, 0.0, 0.0, d);
+        sharpenPlane(cr, nullptr, cr, 1.0, 1.0, 0.0, 0.0, d);
+    }
+    storeOutputPlane(y, out[0], *fmt, false);
+    storeOutputPlane(cb, out[1], *fmt, true);
+    storeOutputPlane(cr, out[2], *fmt, true);
+    return LGCR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TRecon (plugin.cpp:723-990): tReconCreate's defaults and checks, then
+// tReconGetFrame's sequence over raw planes -- per neighbour the reference's
+// blockMatch and applyChromaConsistency (algos.cpp:683-807) and buildLcMap,
+// then guide maps, mutual gate, optional trust mask + plain base, and
+// reconstructChroma with the temporal taps (recon.cpp:642-745), optional
+// collaborativeChromaFilter, output conversion.
+// ---------------------------------------------------------------------------
+namespace {
+
+int tReconSetup(const lgcr_trecon_params *p, const lgcr_format *fmt, int numFrames,
+                LGCRData &d, char *err, size_t errlen) {
+    auto fail = [&](const char *msg) {
+        copyError(err, errlen, msg);
+        return LGCR_E_INVALID;
+    };
+    const bool isFloat = fmt->sample_type == LGCR_ST_FLOAT;
+    if (fmt->color_family != LGCR_CF_YUV || (isFloat && fmt->bits_per_sample != 32) ||
+        (!isFloat && (fmt->bits_per_sample < 8 || fmt->bits_per_sample > 16)) ||
+        fmt->subsampling_w > 1 || fmt->subsampling_h > 1 || fmt->subsampling_w < 0 ||
+        fmt->subsampling_h < 0)
+        return fail("TRecon: planar YUV 444/422/420, 8-16 bit int or 32 bit float");
+    if (fmt->width == 0 || fmt->height == 0 || numFrames == 0)
+        return fail("TRecon: constant dimensions and frame count required");
+    d.outW = fmt->width;
+    d.outH = fmt->height;
+    d.strength = given(p->strength) ? p->strength : 0.8;
+    d.sigma = given(p->sigma) ? p->sigma : 0.01;
+    d.sratio = given(p->sratio) ? p->sratio : 0.15;
+    d.sdb = given(p->sdb) ? p->sdb : 3.0;
+    d.gsigma = given(p->gsigma) ? p->gsigma : 2.5;
+    d.stretch = given(p->stretch) ? p->stretch : 1.0;
+    d.arMargin = given(p->ar) ? p->ar : 0.0;
+    d.ms = given(p->ms) ? p->ms : 1.0;
+    d.trad = given(p->trad) ? p->trad : 1;
+    d.tsearch = given(p->tsearch) ? p->tsearch : 6;
+    d.tsad = given(p->tsad) ? p->tsad : 0.02;
+    if (d.strength < 0.0 || d.strength > 1.0 || d.sigma <= 0.0 || d.sratio <= 0.0 ||
+        d.sdb <= 0.0 || d.stretch < 0.0 || d.gsigma <= 0.0 || d.ms < 0.0 || d.ms > 1.0 ||
+        d.trad < 0 || d.trad > 8 || d.tsearch < 0 || d.tsearch > 64 || d.tsad <= 0.0)
+        return fail("TRecon: invalid parameter range (need 0<=strength<=1, "
+                    "sigma/sratio/sdb/gsigma/tsad>0, stretch>=0, 0<=trad<=8, 0<=tsearch<=64)");
+    d.ridge = given(p->ridge) ? (p->ridge != 0) : true;
+    d.bm = given(p->bm) ? (p->bm != 0) : false;
+    d.sparse = given(p->sparse) ? (p->sparse != 0) : false;
+    d.algo = 2;
+    d.taps = 2 * 3;
+    d.support = 3.0;
+    d.kernel = Kernel::Lanczos;
+    return LGCR_OK;
+}
+
+} // namespace
+
+extern "C" int oracle_trecon_frame(const lgcr_trecon_params *p, const lgcr_format *fmt,
+                                   int numFrames, const lgcr_plane *cur, const lgcr_plane *nbrPlanes,
+                                   int count, const lgcr_plane *out, int chroma_location,
+                                   char *err, size_t errlen) {
+    LGCRData dbase;
+    const int status = tReconSetup(p, fmt, numFrames, dbase, err, errlen);
+    if (status != LGCR_OK)
+        return status;
+    LGCRData dloc = dbase;
+    applyFrameChromaSiting(dloc, *fmt, chroma_location);
+    const LGCRData *d = &dloc;
+    const int sw = cur[0].width, sh = cur[0].height, cw = cur[1].width, ch = cur[1].height;
+    const double rw = double(sw) / cw, rh = double(sh) / ch;
+    Plane y(sw, sh), cb(cw, ch), cr(cw, ch);
+    extractPlanes(cur, *fmt, y, cb, cr, true);
+
+    std::vector<TemporalNbr> nbrs;
+    std::vector<std::unique_ptr<Plane>> store;
+    std::vector<std::vector<int16_t>> mvStoreX, mvStoreY;
+    std::vector<std::vector<float>> confStore;
+    nbrs.reserve(count);
+    mvStoreX.reserve(count);
+    mvStoreY.reserve(count);
+    confStore.reserve(count);
+    if (d->strength > 0.0) {
+        for (int k = 0; k < count; ++k) {
+            auto ny = std::make_unique<Plane>(sw, sh);
+            auto nu = std::make_unique<Plane>(cw, ch);
+            auto nv = std::make_unique<Plane>(cw, ch);
+            extractPlanes(nbrPlanes + 3 * k, *fmt, *ny, *nu, *nv, true);
+            mvStoreX.emplace_back();
+            mvStoreY.emplace_back();
+            confStore.emplace_back();
+            int bw = 0, bh = 0;
+            blockMatch(y, *ny, 16, d->tsearch, float(d->tsad), mvStoreX.back(), mvStoreY.back(),
+                       confStore.back(), bw, bh);
+            applyChromaConsistency(cb, cr, *nu, *nv, sw, sh, 16, mvStoreX.back(),
+                                   mvStoreY.back(), bw, bh, confStore.back());
+            auto lc = std::make_unique<Plane>(buildLcMap(*ny, cw, ch, rw, rh, d->shiftX, d->shiftY));
+            TemporalNbr nb;
+            nb.U = nu.get();
+            nb.V = nv.get();
+            nb.lc = lc.get();
+            nb.mvx = &mvStoreX.back();
+            nb.mvy = &mvStoreY.back();
+            nb.tconf = &confStore.back();
+            nb.bw = bw;
+            nb.bh = bh;
+            nb.block = 16;
+            nbrs.push_back(nb);
+            store.push_back(std::move(ny));
+            store.push_back(std::move(nu));
+            store.push_back(std::move(nv));
+            store.push_back(std::move(lc));
+        }
+    }
+    GuideMaps gm;
+    if (d->strength > 0.0) {
+        gm = buildGuideMaps(y, y, cw, ch, rw, rh, d->shiftX, d->shiftY);
+        if (d->ms > 0.0)
+            gm.ms = buildMutualGate(gm.lc, cb, cr, d->sigma);
+    }
+    storeOutputPlane(y, out[0], *fmt, false);
+
+    Plane cOutU(sw, sh), cOutV(sw, sh);
+    std::vector<uint8_t> mask;
+    if (d->sparse && d->strength > 0.0) {
+        const int dil = int(std::ceil(d->support * std::max(rw, rh))) + 8;
+        mask = buildTrustMask(gm, sw, sh, d->sigma, dil);
+        plainChroma(d, cb, cr, y, gm, sw, sh, cw, ch, cOutU, cOutV);
+    }
+    {
+        ChromaJob job;
+        job.srcU = &cb;
+        job.srcV = &cr;
+        job.srcY = &y;
+        job.gm = &gm;
+        job.dstU = &cOutU;
+        job.dstV = &cOutV;
+        job.srcLumaW = sw;
+        job.srcLumaH = sh;
+        job.rw = rw;
+        job.rh = rh;
+        job.shiftX = d->shiftX;
+        job.shiftY = d->shiftY;
+        job.d = d;
+        if (!mask.empty()) {
+            job.mask = mask.data();
+            job.maskW = sw;
+            job.maskH = sh;
+            job.plainU = &cOutU;
+            job.plainV = &cOutV;
+        }
+        if (!nbrs.empty())
+            job.nbrs = &nbrs;
+        reconstructChroma(job);
+    }
+    if (d->bm)
+        collaborativeChromaFilter(y, cOutU, cOutV, float(d->sigma));
+    storeOutputPlane(cOutU, out[1], *fmt, true);
+    storeOutputPlane(cOutV, out[2], *fmt, true);
+    return LGCR_OK;
+}

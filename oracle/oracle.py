@@ -222,3 +222,80 @@ def recon(planes, chroma_location: int = -1, variant: str = "scalar", bits=None,
     fmt = make_format(planes, bits)
     outs, _ = Recon(fmt, variant, **kwargs).frame(planes, chroma_location)
     return outs
+
+
+def sharpen(planes, bits=None, variant: str = "scalar", **kwargs):
+    """Reference Sharpen of one frame (sharpenCreate + sharpenGetFrame,
+    src/plugin.cpp:14-111); returns the (Y, U, V) outputs. Raises
+    OracleError with the reference's message on invalid arguments."""
+    lib = library(variant)
+    fn = lib.oracle_sharpen_frame
+    fn.argtypes = [ctypes.POINTER(Format)] + [ctypes.c_double] * 5 + [
+        ctypes.POINTER(PlaneDesc), ctypes.POINTER(PlaneDesc), ctypes.c_char_p, ctypes.c_size_t]
+    fn.restype = ctypes.c_int
+    planes = [np.ascontiguousarray(p) for p in planes]
+    outs = [np.zeros_like(p) for p in planes]
+    fmt = make_format(planes, bits)
+    vals = [float(kwargs.pop(k, math.nan)) for k in ("alpha", "sigma", "sratio", "gspatial", "ar")]
+    if kwargs:
+        raise OracleError(f"unknown Sharpen arguments {sorted(kwargs)}")
+    err = ctypes.create_string_buffer(512)
+    if fn(ctypes.byref(fmt), *vals, _planes(planes), _planes(outs), err, 512) != 0:
+        raise OracleError(err.value.decode())
+    return outs
+
+
+class TReconParams(ctypes.Structure):
+    _fields_ = [("strength", ctypes.c_double), ("sigma", ctypes.c_double),
+                ("sratio", ctypes.c_double), ("sdb", ctypes.c_double),
+                ("gsigma", ctypes.c_double), ("stretch", ctypes.c_double),
+                ("ar", ctypes.c_double), ("ridge", ctypes.c_int), ("sparse", ctypes.c_int),
+                ("ms", ctypes.c_double), ("trad", ctypes.c_int), ("tsearch", ctypes.c_int),
+                ("tsad", ctypes.c_double), ("bm", ctypes.c_int)]
+
+
+TRECON_INT_ARGS = ("ridge", "sparse", "trad", "tsearch", "bm")
+
+
+def trecon_params(**kwargs) -> TReconParams:
+    p = TReconParams()
+    for name, ctype in TReconParams._fields_:
+        setattr(p, name, UNSET_INT if ctype is ctypes.c_int else math.nan)
+    for key, value in kwargs.items():
+        if key not in dict(TReconParams._fields_):
+            raise OracleError(f"TRecon: unknown argument {key!r}")
+        if value is not None:
+            setattr(p, key, int(value) if key in TRECON_INT_ARGS else float(value))
+    return p
+
+
+def trecon(cur, nbrs, bits=None, num_frames=None, chroma_location: int = -1,
+           variant: str = "scalar", **kwargs):
+    """Reference TRecon of one frame (tReconCreate + tReconGetFrame,
+    src/plugin.cpp:723-990): `cur` the frame's planes, `nbrs` the planes of
+    its temporal neighbours in temporalFrameNumbers order. Returns the
+    4:4:4 (Y, U, V) outputs."""
+    lib = library(variant)
+    fn = lib.oracle_trecon_frame
+    fn.argtypes = [ctypes.POINTER(TReconParams), ctypes.POINTER(Format), ctypes.c_int,
+                   ctypes.POINTER(PlaneDesc), ctypes.POINTER(PlaneDesc), ctypes.c_int,
+                   ctypes.POINTER(PlaneDesc), ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    fn.restype = ctypes.c_int
+    cur = [np.ascontiguousarray(p) for p in cur]
+    nbrs = [[np.ascontiguousarray(p) for p in f] for f in nbrs]
+    h, w = cur[0].shape
+    outs = [np.zeros((h, w), dtype=cur[0].dtype) for _ in range(3)]
+    fmt = make_format(cur, bits)
+    flat = (PlaneDesc * max(1, 3 * len(nbrs)))()
+    for k, f in enumerate(nbrs):
+        d = _planes(f)
+        for q in range(3):
+            flat[3 * k + q] = d[q]
+    err = ctypes.create_string_buffer(512)
+    params = trecon_params(**kwargs)
+    if num_frames is None:
+        num_frames = 1 + len(nbrs)
+    if fn(ctypes.byref(params), ctypes.byref(fmt), int(num_frames), _planes(cur), flat,
+          len(nbrs), _planes(outs), int(chroma_location), err, 512) != 0:
+        raise OracleError(err.value.decode())
+    return outs

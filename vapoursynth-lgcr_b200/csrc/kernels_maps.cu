@@ -95,6 +95,12 @@ __device__ __forceinline__ void rawStore8(char *row, int x, const uint32_t (&raw
         rawStore<KIND>(row, x + k, raw[k]);
 }
 
+// floatToPlane of a float sample (s * 1.0 + 0.0): the same bits except that
+// a negative zero becomes +0.
+__device__ __forceinline__ uint32_t normalizedFloat(uint32_t raw) {
+    return __float_as_uint(__uint_as_float(raw) + 0.0f);
+}
+
 // Luma: each lane converts 8 consecutive samples (one vector load) in each
 // half of the warp's row segment, both loads issued before any store;
 // unaligned rows take the per-sample path.
@@ -134,8 +140,14 @@ __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, in
                         yw[x + k] = v[k];
                 }
             }
-            if (dst)
+            if (dst) {
+                if (KIND == kF32 && J.lumaNormalize) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        raw[s][k] = normalizedFloat(raw[s][k]);
+                }
                 rawStore8<KIND>(dst, x, raw[s]);
+            }
             continue;
         }
         for (int k = 0; k < 8 && x + k < w; ++k) {
@@ -143,7 +155,7 @@ __device__ __forceinline__ void convertLuma(const FrameJob &J, int y, int xb, in
             if (yw)
                 yw[x + k] = rawToFloat<KIND>(r, scale, 0.0);
             if (dst)
-                rawStore<KIND>(dst, x + k, r);
+                rawStore<KIND>(dst, x + k, (KIND == kF32 && J.lumaNormalize) ? normalizedFloat(r) : r);
         }
     }
 }
@@ -730,7 +742,7 @@ k_gate(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int
     const int tilesX = (w + GT_X - 1) / GT_X;
     const int x0 = (tile % tilesX) * GT_X, y0 = (tile / tilesX) * GT_Y;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const bool dense = !J.sparse ||
+    const bool dense = !J.sparse || J.gateDense ||
         (unsigned long long)J.counters[kCntActiveChroma] * 2ull >= (unsigned long long)w * h;
     if (!dense) {
         // a tile without active samples only stores the zeros of the gate plane

@@ -21,6 +21,7 @@
 // product of two floats is exact in double, so fma(w, u, acc) rounds exactly
 // like the reference's acc += double(w) * u.
 #include "kernels.cuh"
+#include "temporal.cuh"
 #include "plain.cuh"
 
 namespace lgcr_b200 {
@@ -1058,6 +1059,14 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
         tapsSeparable<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
     else
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
+    if (J.tnbCount > 0) {
+        // TRecon: the neighbours' motion-compensated samples follow the
+        // spatial taps in the same accumulators and extend the hull
+        TemporalAcc t{a.u, a.v, a.wsum, a.sumAbs, hMinU, hMaxU, hMinV, hMaxV};
+        t = temporalTaps(J, ox, oy, L0, scx, scy, sigLoc, guideFade, ssRamp, t);
+        a.u = t.u; a.v = t.v; a.wsum = t.wsum; a.sumAbs = t.sumAbs;
+        hMinU = t.mnU; hMaxU = t.mxU; hMinV = t.mnV; hMaxV = t.mxV;
+    }
 
     double valueU, valueV;
     if (a.wsum > 1e-6 && a.wsum >= 0.05 * a.sumAbs) {

@@ -44,6 +44,16 @@ struct RadialView {
     const float *weights;
 };
 
+// One temporal neighbour of a TRecon frame (TemporalNbr, src/lgcr.h:729-736):
+// its chroma and footprint luma map on the chroma grid, and the 16x16 block
+// motion field with its confidence, all in HBM.
+struct TemporalView {
+    const float *U, *V, *lc;           // cw x ch
+    const short *mvx, *mvy;            // bw x bh, luma pixels
+    const float *conf;                 // bw x bh
+    int bw, bh;
+};
+
 struct WeightView {          // polyphase resampler table (luma resize etc.)
     int n, sup;
     const int *start;
@@ -159,6 +169,13 @@ struct __align__(16) FrameJob {
     int bmAnchorsX, bmAnchorsY;
     const int *bmStartsX, *bmStartsY;
     float bmSigma;
+    // TRecon temporal taps (src/recon.cpp:642-745); tnbCount is 0 for Recon
+    const TemporalView *tnb;
+    int tnbCount;
+    int lumaNormalize;                 // float luma copy written as s * 1.0 + 0.0
+    int gateDense;                     // mutual gate on every chroma sample (TRecon)
+    double shiftXd, shiftYd;           // chroma siting, luma units
+    const float *tnwX, *tnwY;          // |sin(pi * frac(mv / r))| per axis, index mv + 64
 };
 
 // ---------------------------------------------------------------------------

@@ -100,6 +100,9 @@ EXPORTS = (
     "lgcr_batch_create", "lgcr_batch_destroy", "lgcr_batch_run",
     "lgcr_batch_launch_count", "lgcr_autotune",
     "lgcr_server_create", "lgcr_server_submit", "lgcr_server_wait", "lgcr_server_destroy",
+    "lgcr_sharpen_params_init", "lgcr_sharpen_create", "lgcr_sharpen_frame",
+    "lgcr_sharpen_destroy", "lgcr_trecon_params_init", "lgcr_trecon_create",
+    "lgcr_trecon_neighbors", "lgcr_trecon_frame", "lgcr_trecon_destroy",
 )
 
 _lib = None
@@ -290,6 +293,165 @@ class Recon:
             raise Error(self.lib.lgcr_last_error().decode())
         if stats:
             return out, st
+        return out
+
+
+class SharpenParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("alpha", "sigma", "sratio", "gspatial", "ar")]
+
+
+SHARPEN_ARGS = ("alpha", "sigma", "sratio", "gspatial", "ar")
+
+
+class Sharpen:
+    """The reference's `lgcr.Sharpen` (sharpenCreate / sharpenGetFrame,
+    src/plugin.cpp:14-111): a 5x5 gated bilateral unsharp mask; same format
+    in and out. Arguments: alpha, sigma, sratio, gspatial, ar."""
+
+    def __init__(self, fmt: Format, **kwargs):
+        self.lib = library()
+        lib = self.lib
+        lib.lgcr_sharpen_create.argtypes = [ctypes.POINTER(SharpenParams), ctypes.POINTER(Format),
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                                            ctypes.c_size_t]
+        lib.lgcr_sharpen_frame.argtypes = [ctypes.c_void_p, ctypes.POINTER(Plane),
+                                           ctypes.POINTER(Plane), ctypes.c_int, ctypes.c_void_p]
+        lib.lgcr_sharpen_destroy.argtypes = [ctypes.c_void_p]
+        params = SharpenParams(*([math.nan] * 5))
+        for key, value in kwargs.items():
+            if key not in SHARPEN_ARGS:
+                raise Error(f"Sharpen: argument {key!r} is not supported")
+            if value is not None:
+                setattr(params, key, float(value))
+        self.fmt = fmt
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        if lib.lgcr_sharpen_create(ctypes.byref(params), ctypes.byref(fmt), ctypes.byref(handle),
+                                   err, 512) != LGCR_OK:
+            raise Error(err.value.decode())
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lgcr_sharpen_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def frame(self, planes, out=None, stream=None):
+        """Sharpen one frame (numpy planes through host memory, or CUDA
+        tensors on `stream` without waiting)."""
+        device = hasattr(planes[0], "data_ptr")
+        if not device:
+            planes = [np.ascontiguousarray(p) for p in planes]
+        if out is None:
+            if device:
+                import torch
+                out = [torch.empty_like(p) for p in planes]
+            else:
+                out = [np.empty_like(p) for p in planes]
+        handle = getattr(stream, "cuda_stream", stream) if stream is not None else None
+        status = self.lib.lgcr_sharpen_frame(self.handle, planes_desc(planes), planes_desc(out),
+                                             LGCR_MEM_DEVICE if device else LGCR_MEM_HOST, handle)
+        if status != LGCR_OK:
+            raise Error(self.lib.lgcr_last_error().decode())
+        return out
+
+
+class TReconParams(ctypes.Structure):
+    _fields_ = [("strength", ctypes.c_double), ("sigma", ctypes.c_double),
+                ("sratio", ctypes.c_double), ("sdb", ctypes.c_double),
+                ("gsigma", ctypes.c_double), ("stretch", ctypes.c_double),
+                ("ar", ctypes.c_double), ("ridge", ctypes.c_int), ("sparse", ctypes.c_int),
+                ("ms", ctypes.c_double), ("trad", ctypes.c_int), ("tsearch", ctypes.c_int),
+                ("tsad", ctypes.c_double), ("bm", ctypes.c_int)]
+
+
+TRECON_INT_ARGS = ("ridge", "sparse", "trad", "tsearch", "bm")
+
+
+class TRecon:
+    """The reference's `lgcr.TRecon` (tReconCreate / tReconGetFrame,
+    src/plugin.cpp:723-990): motion-compensated temporal Recon of a clip of
+    `num_frames` frames. frame(n, get) reconstructs frame n, fetching the
+    planes of frame n and of its neighbours through get(i)."""
+
+    def __init__(self, fmt: Format, num_frames: int, **kwargs):
+        self.lib = library()
+        lib = self.lib
+        lib.lgcr_trecon_create.argtypes = [ctypes.POINTER(TReconParams), ctypes.POINTER(Format),
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.c_char_p, ctypes.c_size_t]
+        lib.lgcr_trecon_frame.argtypes = [ctypes.c_void_p, ctypes.POINTER(Plane),
+                                          ctypes.POINTER(Plane), ctypes.c_int,
+                                          ctypes.POINTER(Plane), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p]
+        lib.lgcr_trecon_neighbors.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.lgcr_trecon_destroy.argtypes = [ctypes.c_void_p]
+        params = TReconParams()
+        for name, ctype in TReconParams._fields_:
+            setattr(params, name, UNSET_INT if ctype is ctypes.c_int else math.nan)
+        for key, value in kwargs.items():
+            if key not in dict(TReconParams._fields_):
+                raise Error(f"TRecon: argument {key!r} is not supported")
+            if value is not None:
+                setattr(params, key, int(value) if key in TRECON_INT_ARGS else float(value))
+        self.fmt = fmt
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        if lib.lgcr_trecon_create(ctypes.byref(params), ctypes.byref(fmt), int(num_frames),
+                                  ctypes.byref(handle), err, 512) != LGCR_OK:
+            raise Error(err.value.decode())
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lgcr_trecon_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def neighbors(self, n: int):
+        buf = (ctypes.c_int * 16)()
+        count = self.lib.lgcr_trecon_neighbors(self.handle, int(n), buf, 16)
+        return list(buf[:count])
+
+    def frame(self, n: int, get, chroma_location: int = -1, out=None, stream=None):
+        """Reconstruct frame n; get(i) returns frame i's (Y, U, V) planes
+        (numpy through host memory, or CUDA tensors on `stream`)."""
+        cur = get(n)
+        nbrs = [get(i) for i in self.neighbors(n)]
+        device = hasattr(cur[0], "data_ptr")
+        h, w = cur[0].shape
+        if not device:
+            cur = [np.ascontiguousarray(p) for p in cur]
+            nbrs = [[np.ascontiguousarray(p) for p in f] for f in nbrs]
+        if out is None:
+            if device:
+                import torch
+                out = [torch.empty((h, w), dtype=cur[0].dtype, device=cur[0].device)
+                       for _ in range(3)]
+            else:
+                out = [np.empty((h, w), dtype=cur[0].dtype) for _ in range(3)]
+        flat = (Plane * max(1, 3 * len(nbrs)))()
+        for k, f in enumerate(nbrs):
+            for q in range(3):
+                flat[3 * k + q] = _plane_desc(f[q])
+        handle = getattr(stream, "cuda_stream", stream) if stream is not None else None
+        status = self.lib.lgcr_trecon_frame(self.handle, planes_desc(cur), flat, len(nbrs),
+                                            planes_desc(out), int(chroma_location),
+                                            LGCR_MEM_DEVICE if device else LGCR_MEM_HOST, handle)
+        if status != LGCR_OK:
+            raise Error(self.lib.lgcr_last_error().decode())
         return out
 
 
