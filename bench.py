@@ -20,6 +20,8 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
   legs         the 1080p algo 2 batch (batched vs per-frame target) and the
                plain 720p, jinc resize and bm+bp configurations: batched and
                per-frame Mpix/s, stage split, roofline
+  filters      Sharpen and TRecon (trad 1) per-frame device path on a 1080p
+               clip, beside the reference's AVX2 build on one thread
   cpu_baseline the reference's AVX2 build on this host's cores (bounded sample)
   serving      the serving configuration's mixed stream (5 frame kinds, algo
                2/4/6, bm on 10 %, 24 streams) as Poisson arrivals at 1.2x the
@@ -366,6 +368,84 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30):
 
 
 # ---------------------------------------------------------------------------
+# the other two filters of the plugin: Sharpen and TRecon on 1080p frames
+# ---------------------------------------------------------------------------
+FILTERS_CLIP = 6                 # frames of the 1080p YUV420P10 clip (TRecon trad 1)
+
+
+def _gen_clip(task):
+    import numpy as np
+    seed, frames = task
+    base = S.make_frame(1920 + 32, 1080 + 32, S.FrameFormat(10, 0, 0), seed=seed)
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(frames):
+        mx, my = int(rng.integers(-3, 4)), int(rng.integers(-3, 4))
+        planes = [p[16 + my:16 + my + 1080, 16 + mx:16 + mx + 1920].astype(np.float64)
+                  for p in base]
+        planes[1] = 0.25 * (planes[1][0::2, 0::2] + planes[1][1::2, 0::2] +
+                            planes[1][0::2, 1::2] + planes[1][1::2, 1::2])
+        planes[2] = 0.25 * (planes[2][0::2, 0::2] + planes[2][1::2, 0::2] +
+                            planes[2][0::2, 1::2] + planes[2][1::2, 1::2])
+        out.append(tuple(np.clip(np.rint(p), 0, 1023).astype(np.uint16) for p in planes))
+    return out
+
+
+def filters_leg(clip, dev, stream, steps, warmup):
+    """Per-frame device-path throughput of Sharpen and TRecon (trad 1, every
+    frame with its two neighbours) on a 1080p YUV420P10 clip resident in HBM,
+    beside the reference's AVX2 build on one host thread for one frame."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    fmt = lgcr.video_format(1920, 1080, 10, 1, 1)
+    dclip = [[torch.from_numpy(p.view(np.int16)).to(dev).view(torch.uint16) for p in f]
+             for f in clip]
+    outs = [torch.empty((1080, 1920), dtype=torch.int16, device=dev).view(torch.uint16)
+            for _ in range(3)]
+    souts = [torch.empty_like(p) for p in dclip[0]]
+    sharpen = lgcr.Sharpen(fmt)
+    trecon = lgcr.TRecon(fmt, len(clip))
+    h = stream.cuda_stream
+
+    def sharpen_pass():
+        for f in dclip:
+            sharpen.frame(f, out=souts, stream=h)
+
+    def trecon_pass():
+        for n in range(len(dclip)):
+            trecon.frame(n, lambda i: dclip[i], out=outs, stream=h)
+
+    res = {}
+    for name, fn in (("sharpen", sharpen_pass), ("trecon", trecon_pass)):
+        for _ in range(max(warmup, 1)):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = a.elapsed_time(b) / (steps * len(dclip))
+        res[name] = {"workload": f"1920x1080 YUV420P10, {len(dclip)}-frame clip" +
+                                 (", trad 1 (two neighbours)" if name == "trecon" else ""),
+                     "ms_per_frame": round(ms, 3),
+                     "mpix_s": round(1920 * 1080 / (ms / 1000) / 1e6, 1)}
+    if O.available("avx2"):
+        t0 = time.perf_counter()
+        O.sharpen(clip[1], 10, variant="avx2")
+        res["sharpen"]["cpu_reference_ms_per_frame"] = round(1000 * (time.perf_counter() - t0), 1)
+        t0 = time.perf_counter()
+        O.trecon(clip[1], [clip[0], clip[2]], 10, len(clip), variant="avx2")
+        res["trecon"]["cpu_reference_ms_per_frame"] = round(1000 * (time.perf_counter() - t0), 1)
+        res["cpu_reference"] = "reference AVX2 build (oracle/_ref), one host thread, one frame"
+    sharpen.close()
+    trecon.close()
+    return res
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 FORMATS = {"420P8": S.YUV420P8, "420P10": S.YUV420P10, "420P16": S.YUV420P16,
@@ -590,6 +670,10 @@ def our_arm(args):
     frames = generate(specs)                      # before CUDA init (spawn pools)
     legs = leg_specs(rank) if not args.no_legs else {}
     leg_frames = generate_legs(legs)
+    clip = None
+    if not args.no_legs:
+        with mp.get_context("spawn").Pool(1) as pool:
+            clip = pool.map(_gen_clip, [(R.frame_seed(11000, rank, 0), FILTERS_CLIP)])[0]
     cpu_frames = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_frames = frames
@@ -826,6 +910,9 @@ def our_arm(args):
             b.close()
             del lf
         result["legs"] = out_legs
+
+    if clip is not None:
+        result["filters"] = filters_leg(clip, dev, stream, max(3, min(args.steps, 10)), args.warmup)
 
     if rank == 0 and args.serve_requests > 0:
         # content of the serving stream (spawned workers: safe after CUDA init)
