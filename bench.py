@@ -12,6 +12,7 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
   e2e          same metric through the per-frame C ABI (lgcr_recon_frame) with
                pinned host planes: H2D, run, D2H inside the timed region, one
                calling host thread per core (at most 16) like fmParallel
+               (e2e_pageable: the same with pageable host planes)
   per_frame    device-resident per-frame path (one lgcr_recon_frame per frame)
   roofline     dominant stage: algorithmic bytes of the frames its launch
                processes (9 B per output pixel for 10-bit 4:2:0 -> 4:4:4) / its
@@ -783,7 +784,7 @@ def our_arm(args):
 
     e2e_threads = args.e2e_threads or min(16, cpu_threads())
 
-    def e2e_pass(nthreads=e2e_threads):
+    def e2e_pass(nthreads=e2e_threads, ins=pinned_in, outs=pinned_out):
         lock = threading.Lock()
         queue = list(range(len(specs)))
 
@@ -795,7 +796,7 @@ def our_arm(args):
                     i = queue.pop(0)
                 f = head_filters[i]
                 t0 = time.perf_counter()
-                f.frame(pinned_in[i], -1, out=pinned_out[i])
+                f.frame(ins[i], -1, out=outs[i])
                 with lock:
                     latencies.append(1000 * (time.perf_counter() - t0))
 
@@ -818,6 +819,20 @@ def our_arm(args):
     e2e_s = time.perf_counter() - t0
     e2e_s = R.max_over_ranks(e2e_s, dev)
     e2e_value = out_pixels * world * args.steps / e2e_s / 1e6
+    e2e_latencies = list(latencies)
+    # the same through pageable host buffers (how a VapourSynth host holds its
+    # frames): the library stages them in pinned memory of its own
+    page_in = [[np.array(p) for p in planes] for planes in frames]
+    page_out = [[None] + [np.empty((s["height"], s["width"]), np.uint16) for _ in range(2)]
+                for s in specs]
+    e2e_pass(ins=page_in, outs=page_out)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_pass(ins=page_in, outs=page_out)
+    torch.cuda.synchronize(dev)
+    e2e_page_s = R.max_over_ranks(time.perf_counter() - t0, dev)
+    latencies[:] = e2e_latencies
     out_bytes_e2e = sum(2 * s["width"] * s["height"] * 2 for s in specs)   # U, V (luma shared)
 
     # roofline of the dominant stage, with the guided stage's FP32 side
@@ -867,6 +882,9 @@ def our_arm(args):
                        if latencies else None, "per": "frame, e2e host path"},
         "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "host_threads": e2e_threads,
                 "h2d_bytes_per_step": int(head.in_bytes), "d2h_bytes_per_step": int(out_bytes_e2e)},
+        "e2e_pageable": {"value": round(out_pixels * world * args.steps / e2e_page_s / 1e6, 2),
+                         "unit": "Mpix/s", "host_threads": e2e_threads,
+                         "buffers": "pageable numpy planes, staged by the library"},
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": rl,
         "clocks": clocks,

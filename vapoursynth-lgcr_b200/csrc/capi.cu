@@ -46,6 +46,25 @@ cudaEvent_t threadDoneEvent() {
     return ev;
 }
 
+// Page-locked (or otherwise device-accessible) host memory: the DMA engine
+// reads or writes it directly.
+bool pinnedHost(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
+// Host rows between a strided caller plane and a packed staging buffer.
+void copyRows(void *dst, size_t dpitch, const void *src, size_t spitch, size_t rowBytes,
+              size_t rows) {
+    for (size_t r = 0; r < rows; ++r)
+        std::memcpy(static_cast<char *>(dst) + r * dpitch,
+                    static_cast<const char *>(src) + r * spitch, rowBytes);
+}
+
 bool checkPlane(const lgcr_plane &p, int w, int h, int bps, bool allowNull) {
     if (!p.data)
         return allowNull;
@@ -151,10 +170,24 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         cudaEventSynchronize(ws->done);
     t.ws = ws;
     cudaError_t e = cudaSuccess;
+    bool pageableOut[3] = {false, false, false};
     if (memory == LGCR_MEM_HOST) {
         for (int i = 0; i < 3; ++i) {
-            e = copyPlane(ws->stageIn[i], ws->stageInPitch[i], in[i].data, in[i].stride,
-                          size_t(in[i].width) * bps, in[i].height, cudaMemcpyHostToDevice, s);
+            const size_t rowBytes = size_t(in[i].width) * bps, rows = in[i].height;
+            if (pinnedHost(in[i].data)) {
+                e = copyPlane(ws->stageIn[i], ws->stageInPitch[i], in[i].data, in[i].stride,
+                              rowBytes, rows, cudaMemcpyHostToDevice, s);
+            } else {
+                // pageable caller memory (a VapourSynth frame): stage it in this
+                // workspace's pinned buffer, then one DMA
+                if (!ws->pinnedIn[i])
+                    e = cudaHostAlloc(&ws->pinnedIn[i], rowBytes * rows, cudaHostAllocDefault);
+                if (e == cudaSuccess) {
+                    copyRows(ws->pinnedIn[i], rowBytes, in[i].data, in[i].stride, rowBytes, rows);
+                    e = copyPlane(ws->stageIn[i], ws->stageInPitch[i], ws->pinnedIn[i], rowBytes,
+                                  rowBytes, rows, cudaMemcpyHostToDevice, s);
+                }
+            }
             if (e != cudaSuccess) break;
             t.in[i] = { ws->stageIn[i], (ptrdiff_t)ws->stageInPitch[i], in[i].width, in[i].height };
             t.out[i] = { ws->stageOut[i], (ptrdiff_t)ws->stageOutPitch[i], F.p.outW, F.p.outH };
@@ -182,8 +215,18 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
             if (!out[i].data)
                 continue;
-            e = copyPlane(out[i].data, out[i].stride, ws->stageOut[i], ws->stageOutPitch[i],
-                          size_t(F.p.outW) * bps, F.p.outH, cudaMemcpyDeviceToHost, s);
+            const size_t rowBytes = size_t(F.p.outW) * bps, rows = F.p.outH;
+            if (pinnedHost(out[i].data)) {
+                e = copyPlane(out[i].data, out[i].stride, ws->stageOut[i], ws->stageOutPitch[i],
+                              rowBytes, rows, cudaMemcpyDeviceToHost, s);
+                continue;
+            }
+            if (!ws->pinnedOut[i])
+                e = cudaHostAlloc(&ws->pinnedOut[i], rowBytes * rows, cudaHostAllocDefault);
+            if (e == cudaSuccess)
+                e = copyPlane(ws->pinnedOut[i], rowBytes, ws->stageOut[i], ws->stageOutPitch[i],
+                              rowBytes, rows, cudaMemcpyDeviceToHost, s);
+            pageableOut[i] = true;
         }
     }
     unsigned long long counters[kCntCount] = {};
@@ -193,7 +236,9 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         e = cudaEventRecord(ws->done, s);
     ws->used = true;
     const FrameJob J = *ws->hJob;
-    F.release(ws);
+    const bool holdStaging = pageableOut[0] || pageableOut[1] || pageableOut[2];
+    if (!holdStaging)
+        F.release(ws);
     // wait on a blocking-sync event of this thread recorded after the frame's
     // last operation: the calling thread sleeps instead of spinning on a core
     if (e == cudaSuccess && (memory == LGCR_MEM_HOST || stats)) {
@@ -201,6 +246,17 @@ int lgcr_recon_frame(lgcr_recon *h, const lgcr_plane in[3], const lgcr_plane out
         e = fin ? cudaEventRecord(fin, s) : cudaStreamSynchronize(s);
         if (fin && e == cudaSuccess)
             e = cudaEventSynchronize(fin);
+    }
+    if (holdStaging) {
+        // pageable outputs leave the workspace's pinned buffers only now; the
+        // workspace returns to the pool afterwards
+        for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+            if (pageableOut[i]) {
+                const size_t rowBytes = size_t(F.p.outW) * bps;
+                copyRows(out[i].data, out[i].stride, ws->pinnedOut[i], rowBytes, rowBytes,
+                         F.p.outH);
+            }
+        F.release(ws);
     }
     if (e != cudaSuccess)
         return cudaFail(e, "lgcr_recon_frame");

@@ -110,6 +110,11 @@ struct Workspace {
     cudaEvent_t done = nullptr;
     bool used = false;
     bool hostStaging = false;           // has the host-buffer staging planes
+    // pinned host copies of the planes for callers whose buffers are pageable
+    // (allocated on first use): the DMA then runs from/to page-locked memory
+    // and concurrent frames do not share the driver's staging buffer
+    void *pinnedIn[3] = {nullptr, nullptr, nullptr};
+    void *pinnedOut[3] = {nullptr, nullptr, nullptr};
     ~Workspace();
 };
 

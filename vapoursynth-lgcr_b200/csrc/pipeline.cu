@@ -40,6 +40,12 @@ bool DeviceArena::commit() {
 Workspace::~Workspace() {
     if (done)
         cudaEventDestroy(done);
+    for (int i = 0; i < 3; ++i) {
+        if (pinnedIn[i])
+            cudaFreeHost(pinnedIn[i]);
+        if (pinnedOut[i])
+            cudaFreeHost(pinnedOut[i]);
+    }
     if (hJob)
         cudaFreeHost(hJob);
 }
