@@ -27,7 +27,8 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
   serving      the serving configuration's mixed stream (5 frame kinds, algo
                2/4/6, bm on 10 %, 24 streams) as Poisson arrivals at 1.2x the
                per-frame path's capacity into the continuous-batching server
-               (8 GB budget): throughput and p50/p99/p99.9 latency
+               (8 GB budget): throughput and p50/p99/p99.9 latency, plus an
+               arrival-rate sweep naming the highest rate with p99 <= 100 ms
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -273,10 +274,11 @@ def serve_requests(n, seed=4000):
              int(rng.choice([2, 4, 6])), bool(rng.random() < 0.1)) for _ in range(n)]
 
 
-def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30):
+def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30,
+                sweep_factors=(0.5, 0.8, 1.0, 1.5), sweep_requests=600):
     """Poisson arrivals at 1.2x the per-frame path's capacity into the
-    continuous-batching server; latency from submit to completion on the
-    server's clock."""
+    continuous-batching server, then shorter streams at other rates; latency
+    from submit to completion on the server's clock."""
     import numpy as np
     import torch
     import lgcr
@@ -324,48 +326,67 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30):
     for (s, k, algo, bm) in sample:
         filt(k, algo, bm).frame(pins[(k, s % SERVE_SEEDS)], -1, out=out_set(k)[1])
     plain_fps = len(sample) / (time.perf_counter() - t0)
-    rate = 1.2 * plain_fps
-    arrivals = np.cumsum(np.random.default_rng(4001).exponential(1.0 / rate, len(reqs)))
-    server = lgcr.Server(budget_bytes=budget, max_batch=max_batch, lanes=lanes,
-                         queue_capacity=len(reqs) + 1)
-    tickets = [None] * len(reqs)
-    owner = {}                     # (kind, ring slot) -> request index using it
-    infos = [None] * len(reqs)
-    pixels = 0
-    start = time.perf_counter()
-    for i, (s, k, algo, bm) in enumerate(reqs):
-        delay = start + arrivals[i] - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        slot, out = out_set(k)
-        prev = owner.get((k, slot))
-        if prev is not None and infos[prev] is None:
-            infos[prev] = server.wait(tickets[prev])[1]      # ring slot still in flight
-        owner[(k, slot)] = i
-        f = filt(k, algo, bm)
-        tickets[i] = server.submit(f, pins[(k, s % SERVE_SEEDS)], out)
-        if tickets[i] < 0:
-            raise RuntimeError(f"serving submit failed: {tickets[i]}")
-        pixels += f.out_w * f.out_h
-    for i in range(len(reqs)):
-        if infos[i] is None:
-            infos[i] = server.wait(tickets[i])[1]
-    server.close()
-    lat = np.array([inf.done_ms - inf.submit_ms for inf in infos])
-    span_ms = max(inf.done_ms for inf in infos) - min(inf.submit_ms for inf in infos)
-    bad = sum(1 for inf in infos if inf.status != 0)
-    return {
-        "requests": len(reqs), "failed": bad, "streams": SERVE_STREAMS,
+
+    def run_stream(stream_reqs, rate, seed):
+        """Poisson arrivals at `rate` frames/s; per-request latency from submit
+        to completion on the server's clock."""
+        arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, len(stream_reqs)))
+        server = lgcr.Server(budget_bytes=budget, max_batch=max_batch, lanes=lanes,
+                             queue_capacity=len(stream_reqs) + 1)
+        tickets = [None] * len(stream_reqs)
+        owner = {}                     # (kind, ring slot) -> request index using it
+        infos = [None] * len(stream_reqs)
+        pixels = 0
+        start = time.perf_counter()
+        for i, (st, k, algo, bm) in enumerate(stream_reqs):
+            delay = start + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            slot, out = out_set(k)
+            prev = owner.get((k, slot))
+            if prev is not None and infos[prev] is None:
+                infos[prev] = server.wait(tickets[prev])[1]      # ring slot still in flight
+            owner[(k, slot)] = i
+            f = filt(k, algo, bm)
+            tickets[i] = server.submit(f, pins[(k, st % SERVE_SEEDS)], out)
+            if tickets[i] < 0:
+                raise RuntimeError(f"serving submit failed: {tickets[i]}")
+            pixels += f.out_w * f.out_h
+        for i in range(len(stream_reqs)):
+            if infos[i] is None:
+                infos[i] = server.wait(tickets[i])[1]
+        server.close()
+        lat = np.array([inf.done_ms - inf.submit_ms for inf in infos])
+        span_ms = max(inf.done_ms for inf in infos) - min(inf.submit_ms for inf in infos)
+        return {
+            "arrival_rate_fps": round(rate, 1), "requests": len(stream_reqs),
+            "failed": sum(1 for inf in infos if inf.status != 0),
+            "throughput_fps": round(len(stream_reqs) / (span_ms / 1000), 1),
+            "throughput_mpix_s": round(pixels / (span_ms / 1000) / 1e6, 1),
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                           "p99": round(float(np.percentile(lat, 99)), 3),
+                           "p99.9": round(float(np.percentile(lat, 99.9)), 3)}}
+
+    main = run_stream(reqs, 1.2 * plain_fps, 4001)
+    # arrival-rate sweep: the highest rate whose p99 stays under 100 ms is the
+    # sustainable throughput of this mixed stream
+    sweep = []
+    for factor in sweep_factors:
+        r = run_stream(reqs[:sweep_requests], factor * plain_fps, 4100 + int(100 * factor))
+        r["rate_factor"] = factor
+        sweep.append(r)
+    ok = [r for r in sweep if r["latency_ms"]["p99"] <= 100.0 and r["failed"] == 0]
+    best = max(ok, key=lambda r: r["throughput_mpix_s"]) if ok else None
+    return dict(main, **{
+        "streams": SERVE_STREAMS,
         "kinds": [kd[0] for kd in SERVE_KINDS], "algos": [2, 4, 6], "bm_fraction": 0.1,
         "content": f"{SERVE_SEEDS} seeded frames per kind shared by the streams",
-        "per_frame_capacity_fps": round(plain_fps, 1), "arrival_rate_fps": round(rate, 1),
-        "throughput_fps": round(len(reqs) / (span_ms / 1000), 1),
-        "throughput_mpix_s": round(pixels / (span_ms / 1000) / 1e6, 1),
-        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
-                       "p99": round(float(np.percentile(lat, 99)), 3),
-                       "p99.9": round(float(np.percentile(lat, 99.9)), 3)},
+        "per_frame_capacity_fps": round(plain_fps, 1),
         "server": {"lanes": lanes, "max_batch": max_batch, "budget_gb": budget / 2 ** 30},
-    }
+        "sweep": sweep,
+        "sustainable_p99_under_100ms": ({"arrival_rate_fps": best["arrival_rate_fps"],
+                                         "throughput_mpix_s": best["throughput_mpix_s"],
+                                         "latency_ms": best["latency_ms"]} if best else None)})
 
 
 # ---------------------------------------------------------------------------
