@@ -758,20 +758,54 @@ __device__ __forceinline__ float pointLuma(const FrameJob &J, int x, int y) {
 // LGF regression per chroma sample: 5x5 sums of {l, l^2, u, l*u, v, l*v}
 // with l the point-sampled luma; conf = var/(var+eps) (x cedge fade), then
 // the mutual-structure fade. Integer output: all samples; float: ROI only.
+//
+// A block stages its tile's point-sampled luma (computed once per sample,
+// not once per window that covers it) and U, V with a 2-sample clamped halo
+// in shared memory; each thread then sums its clipped 5x5 window from there
+// in the same raster order, so the sums are the reference's. Tiles without
+// an ROI sample only store the maps' zeros.
+constexpr int kLgfTile = 1024;               // (bx + 4) * (by + 4) of every block shape used
+
 __global__ void __launch_bounds__(256)
 k_lgf(LGCR_STAGE_ARGS) {
+    __shared__ float sL[kLgfTile], sU[kLgfTile], sV[kLgfTile];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
-    int x, y;
-    tile32x8(blockIdx.x - tileStart[f], J.cw, x, y);
     const int w = J.cw, h = J.ch;
-    if (x >= w || y >= h)
-        return;
-    const size_t o = (size_t)y * w + x;
-    if (J.lgfRoiOnly && J.roi[o] == 0) {
+    const int bx = blockDim.x, by = blockDim.y;
+    const int tile = blockIdx.x - tileStart[f];
+    const int tilesX = (w + bx - 1) / bx;
+    const int x0 = (tile % tilesX) * bx, y0 = (tile / tilesX) * by;
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    const bool inside = x < w && y < h;
+    const size_t o = inside ? (size_t)y * w + x : 0;
+    const bool work = inside && (!J.lgfRoiOnly || J.roi[o] != 0);
+    const int lx = bx + 4, ly = by + 4;
+    const bool staged = lx * ly <= kLgfTile;
+    if (!__syncthreads_or(work)) {
         // outside the ROI the maps hold zeros (buildLGFMaps fills them before
         // the ROI pass, recon.cpp:1541-1548); the blend reads them wherever
         // w2 or w3 reaches 1e-4, which includes samples outside the ROI
+        if (inside) {
+            const size_t C = (size_t)w * h;
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                J.lgf[k * C + o] = 0.0f;
+        }
+        return;
+    }
+    if (staged) {
+        for (int k = threadIdx.y * bx + threadIdx.x; k < lx * ly; k += bx * by) {
+            const int px = iclamp(x0 - 2 + k % lx, 0, w - 1), py = iclamp(y0 - 2 + k / lx, 0, h - 1);
+            sL[k] = pointLuma(J, px, py);
+            sU[k] = ldf(J.U + (size_t)py * w + px);
+            sV[k] = ldf(J.V + (size_t)py * w + px);
+        }
+    }
+    __syncthreads();
+    if (!inside)
+        return;
+    if (!work) {
         const size_t C = (size_t)w * h;
 #pragma unroll
         for (int k = 0; k < 6; ++k)
@@ -781,12 +815,23 @@ k_lgf(LGCR_STAGE_ARGS) {
     const int top = max(0, y - 2), bottom = min(h - 1, y + 2);
     const int left = max(0, x - 2), right = min(w - 1, x + 2);
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int py = top; py <= bottom; ++py)
-        for (int px = left; px <= right; ++px) {
-            const double ly = pointLuma(J, px, py);
-            const double u = ldf(J.U + (size_t)py * w + px), v = ldf(J.V + (size_t)py * w + px);
-            s[0] += ly; s[1] += ly * ly; s[2] += u; s[3] += ly * u; s[4] += v; s[5] += ly * v;
+    if (staged) {
+        for (int py = top; py <= bottom; ++py) {
+            const int r = (py - y0 + 2) * lx - x0 + 2;
+            for (int px = left; px <= right; ++px) {
+                const double lv = sL[r + px];
+                const double u = sU[r + px], v = sV[r + px];
+                s[0] += lv; s[1] += lv * lv; s[2] += u; s[3] += lv * u; s[4] += v; s[5] += lv * v;
+            }
         }
+    } else {
+        for (int py = top; py <= bottom; ++py)
+            for (int px = left; px <= right; ++px) {
+                const double lv = pointLuma(J, px, py);
+                const double u = ldf(J.U + (size_t)py * w + px), v = ldf(J.V + (size_t)py * w + px);
+                s[0] += lv; s[1] += lv * lv; s[2] += u; s[3] += lv * u; s[4] += v; s[5] += lv * v;
+            }
+    }
     const int n = (right - left + 1) * (bottom - top + 1);
     const double eps = J.lgfEps;
     const double meanY = s[0] / n;
