@@ -1255,19 +1255,57 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
     storeLuma(J, x, y, (float)acc);
 }
 
-__global__ void k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart,
-                              int njobs) {
+// 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x8
+// block of output pixels stages the clamped input rows and columns its
+// windows cover and the kernel's LUT in shared memory (when they fit), so
+// the sup x sup taps read shared memory; the tap weights and the FP64
+// accumulation follow the reference's order and arithmetic.
+constexpr int kRadialTileMax = 6144;         // staged luma samples per block
+constexpr int kRadialLutMax = 4096;          // staged LUT entries
+
+__device__ __forceinline__ float lutLookupShared(const float *lut, int n, float idx) {
+    int i0 = (int)idx;
+    i0 = iclamp(i0, 0, n - 2);
+    const float fr = smin(idx - (float)i0, 1.0f);
+    const float a = lut[i0];
+    return a + (lut[i0 + 1] - a) * fr;
+}
+
+__global__ void __launch_bounds__(256)
+k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    __shared__ float sY[kRadialTileMax];
+    __shared__ float sLut[kRadialLutMax];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
-    int ox, oy;
-    tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
-    if (ox >= J.W || oy >= J.H)
-        return;
+    const int tile = blockIdx.x - tileStart[f];
+    const int tilesX = (J.W + 31) / 32;
+    const int bx0 = (tile % tilesX) * 32, by0 = (tile / tilesX) * 8;
+    const int ox = bx0 + threadIdx.x, oy = by0 + threadIdx.y;
     const double sx = (double)J.sw / J.W, sy = (double)J.sh / J.H;
     const double widen = fmax(1.0, fmax(sx, sy));
     const float invW = (float)(1.0 / widen);
     const int radius = (int)ceil(J.support * widen);
     const int sup = 2 * radius;
+    // the block's footprint: first tap of its first pixel to last tap of its
+    // last pixel, per axis (the first tap grows with the output index)
+    const int bxLast = min(bx0 + 31, J.W - 1), byLast = min(by0 + 7, J.H - 1);
+    const int fx0 = (int)ceil((bx0 + 0.5) * sx - 0.5 - radius);
+    const int fy0 = (int)ceil((by0 + 0.5) * sy - 0.5 - radius);
+    const int fw = (int)ceil((bxLast + 0.5) * sx - 0.5 - radius) + sup - fx0;
+    const int fh = (int)ceil((byLast + 0.5) * sy - 0.5 - radius) + sup - fy0;
+    const bool tileStaged = fw * fh <= kRadialTileMax;
+    const bool lutStaged = J.lutN <= kRadialLutMax;
+    const int nt = blockDim.x * blockDim.y, t = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tileStaged)
+        for (int k = t; k < fw * fh; k += nt)
+            sY[k] = ldf(J.Y + (size_t)iclamp(fy0 + k / fw, 0, J.sh - 1) * J.sw +
+                        iclamp(fx0 + k % fw, 0, J.sw - 1));
+    if (lutStaged)
+        for (int k = t; k < J.lutN; k += nt)
+            sLut[k] = ldf(J.lut + k);
+    __syncthreads();
+    if (ox >= J.W || oy >= J.H)
+        return;
     const double cy = (oy + 0.5) * sy - 0.5;
     const int y0 = (int)ceil(cy - radius);
     const double cx = (ox + 0.5) * sx - 0.5;
@@ -1277,11 +1315,14 @@ __global__ void k_luma_radial(const FrameJob *__restrict__ jobs, const int *__re
         const int ty = iclamp(y0 + j, 0, J.sh - 1);
         const float dy = (float)((y0 + j - cy) * invW);
         const float *row = J.Y + (size_t)ty * J.sw;
+        const int srow = (y0 + j - fy0) * fw - fx0;
         for (int i = 0; i < sup; ++i) {
-            const int tx = iclamp(x0 + i, 0, J.sw - 1);
             const float dx = (float)((x0 + i - cx) * invW);
-            const float w = lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
-            acc = fma((double)w, (double)ldf(row + tx), acc);
+            const float r = sqrtf(dx * dx + dy * dy) * J.lutScale;
+            const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r)
+                                      : lutLookupDev(J.lut, J.lutN, r);
+            const float v = tileStaged ? sY[srow + x0 + i] : ldf(row + iclamp(x0 + i, 0, J.sw - 1));
+            acc = fma((double)w, (double)v, acc);
             wsum += (double)w;
         }
     }
