@@ -685,6 +685,56 @@ def roofline_of(stage_ms, kinds, algo_bytes, peaks, steps_note):
             "stage_timing": steps_note}
 
 
+def leg_only(args):
+    """Profiler captures: run one leg alone (a configuration's batch, or the
+    Sharpen / TRecon clip) for `steps` graph replays after `warmup` and print
+    its time and stage split."""
+    global lgcr
+    rank = 0
+    if args.leg in ("sharpen", "trecon"):
+        with mp.get_context("spawn").Pool(1) as pool:
+            clip = pool.map(_gen_clip, [(R.frame_seed(11000, rank, 0), FILTERS_CLIP)])[0]
+    else:
+        legs = leg_specs(rank)
+        if args.leg not in legs:
+            raise SystemExit(f"unknown leg {args.leg!r}; one of {sorted(legs)} or sharpen, trecon")
+        leg = legs[args.leg]
+        if leg.get("reuse_headline"):
+            specs = [s for s in frame_specs(rank, args.frames) if s["width"] == 1920]
+            planes_list = generate(specs)
+        else:
+            planes_list = generate_legs({args.leg: leg})[args.leg]
+    import torch
+    import lgcr as _lgcr
+    lgcr = _lgcr
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    lib = lgcr.library()
+    lib.lgcr_batch_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.lgcr_batch_stage_times.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.lgcr_stage_name.restype = ctypes.c_char_p
+    if args.leg in ("sharpen", "trecon"):
+        res = filters_leg(clip, dev, stream, args.steps, args.warmup)
+        print(json.dumps({"leg": args.leg, **res[args.leg]}))
+        return 0
+    filters = [lgcr.Recon(lgcr.format_of(p, 10 if leg.get("reuse_headline") else None),
+                          **leg["filter"]) for p in planes_list]
+    b = BatchLeg(lib, dev, stream, filters, planes_list)
+    for _ in range(max(args.warmup, 1)):
+        b.run(1)
+    torch.cuda.synchronize(dev)
+    ms = b.timed(lambda: b.run(1), args.steps)
+    stage_ms = b.stage_split(1)
+    b.close()
+    print(json.dumps({"leg": args.leg, "frames": len(filters),
+                      "ms_per_step": round(ms / args.steps, 3),
+                      "mpix_s": round(b.out_pixels * args.steps / (ms / 1000) / 1e6, 1),
+                      "stage_ms_per_step": {k: round(v, 3) for k, v in
+                                            sorted(stage_ms.items(), key=lambda kv: -kv[1])}}))
+    return 0
+
+
 def our_arm(args):
     global lgcr
     rank, world, local = R.rank_info()
@@ -997,12 +1047,17 @@ def main():
                     help="time the batched form only (profiler captures)")
     ap.add_argument("--no-legs", action="store_true",
                     help="skip the north-star and per-configuration legs")
+    ap.add_argument("--leg", default="",
+                    help="run one leg alone (profiler captures): a configuration leg's "
+                         "name, sharpen or trecon")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # one process per GPU: start the replicas under torchrun
         return R.relaunch(os.path.abspath(__file__), sys.argv[1:], args.gpus)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.leg:
+        return leg_only(args)
     return our_arm(args)
 
 
