@@ -718,6 +718,8 @@ def leg_only(args):
         res = filters_leg(clip, dev, stream, args.steps, args.warmup)
         print(json.dumps({"leg": args.leg, **res[args.leg]}))
         return 0
+    if args.leg_frames > 0:
+        planes_list = planes_list[:args.leg_frames]
     filters = [lgcr.Recon(lgcr.format_of(p, 10 if leg.get("reuse_headline") else None),
                           **leg["filter"]) for p in planes_list]
     b = BatchLeg(lib, dev, stream, filters, planes_list)
@@ -1050,6 +1052,8 @@ def main():
     ap.add_argument("--leg", default="",
                     help="run one leg alone (profiler captures): a configuration leg's "
                          "name, sharpen or trecon")
+    ap.add_argument("--leg-frames", type=int, default=0,
+                    help="with --leg: keep only the first N frames of the leg (small captures)")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # one process per GPU: start the replicas under torchrun
