@@ -382,7 +382,8 @@ extern "C" int lgcr_autotune(const lgcr_batch_item *items, int count, void *stre
         double best = 1e300;
         int bestV = guidedVariant();
         std::string line = "reconstructChroma:";
-        for (int v = 0; v < 2 && guidedStage >= 0 && status == LGCR_OK; ++v) {
+        static const char *names[3] = {"2-blocks", "3-blocks", "staged"};
+        for (int v = 0; v < 3 && guidedStage >= 0 && status == LGCR_OK; ++v) {
             setGuidedVariant(v);
             status = lgcr_batch_run(b, items, count, stream, 0);
             lgcr_batch_stage_times(b, nullptr, nullptr, 1);
@@ -392,13 +393,13 @@ extern "C" int lgcr_autotune(const lgcr_batch_item *items, int count, void *stre
             if (ms[guidedStage] <= 0.0)
                 break;
             char buf[64];
-            std::snprintf(buf, sizeof(buf), " %d-blocks=%.3fms", v ? 3 : 2, ms[guidedStage] / 2);
+            std::snprintf(buf, sizeof(buf), " %s=%.3fms", names[v], ms[guidedStage] / 2);
             line += buf;
             if (ms[guidedStage] < best) { best = ms[guidedStage]; bestV = v; }
         }
         setGuidedVariant(bestV);
         if (best < 1e300)
-            text += line + (bestV ? " -> 3 blocks/SM\n" : " -> 2 blocks/SM\n");
+            text += line + " -> " + names[bestV] + "\n";
     }
     lgcr_batch_destroy(b);
     if (report && reportlen) {

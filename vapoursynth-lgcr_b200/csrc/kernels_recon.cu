@@ -735,9 +735,14 @@ __device__ __forceinline__ void accumulate(Acc &a, float w, double2 p) {
 // columns are processed in pairs with tapCore's arithmetic on packed pairs
 // (range checks of the reciprocals hoisted by the caller), and each active
 // tap is accumulated in FP64 in tap order.
-template <int SUP>
+// lc0/uv0 point at the window's tap (0, 0); rows are `stride` samples apart.
+// SH: the window was staged in shared memory by the warp (plain loads);
+// otherwise it is read from the planes in global memory.
+template <int SUP, bool SH>
 __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
-                                              const float *wyp, uint32_t mx, uint32_t my, Acc &a) {
+                                              const float *wyp, uint32_t mx, uint32_t my,
+                                              const float *lc0, const double2 *uv0, int stride,
+                                              Acc &a) {
     constexpr int NP = SUP / 2;
     f32x2 dxnx[NP], dxny[NP], wxv[NP];
     if (SUP % 4 == 0) {
@@ -769,8 +774,8 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
     for (int j = 0; j < SUP; ++j) {
         if (!((my >> j) & 1u))
             continue;
-        const float *lrow = c.lc + (size_t)(ty0 + j) * c.cw + tx0;
-        const double2 *uvrow = c.uv + (size_t)(ty0 + j) * c.cw + tx0;
+        const float *lrow = lc0 + (size_t)j * stride;
+        const double2 *uvrow = uv0 + (size_t)j * stride;
         const float wy = __ldg(wyp + j);
         const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
         const f32x2 wyy = pk2(wy, wy);
@@ -778,8 +783,10 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
             const int i = 2 * q;
-            const double2 p0 = __ldg(uvrow + i), p1 = __ldg(uvrow + i + 1);
-            const f32x2 dL = sub2(pk2(ldf(lrow + i), ldf(lrow + i + 1)), L0);
+            const double2 p0 = SH ? uvrow[i] : __ldg(uvrow + i);
+            const double2 p1 = SH ? uvrow[i + 1] : __ldg(uvrow + i + 1);
+            const float l0 = SH ? lrow[i] : ldf(lrow + i), l1 = SH ? lrow[i + 1] : ldf(lrow + i + 1);
+            const f32x2 dL = sub2(pk2(l0, l1), L0);
             const f32x2 simRaw = rcp2(add2(one, mul2(mul2(dL, dL), invS)), one);
             const f32x2 sim = sub2(one, mul2(fade, sub2(one, simRaw)));
             const f32x2 dp = add2(dxnx[q], dyny);
@@ -860,7 +867,18 @@ struct Guided {
     bool hasDir;
 };
 
-__device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy) {
+// A warp's guided-tap window staged in shared memory: kStageRows x
+// kStageCols chroma samples (lc and the FP64 (u, v) pair) starting at chroma
+// (tx0, ty0), the same rows for every pixel of the warp.
+constexpr int kStageRows = 8, kStageCols = 40;
+struct StagedWindow {
+    const float *lc;
+    const double2 *uv;
+    int tx0, ty0;
+};
+
+__device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
+                                              const StagedWindow *win) {
     const AxisView &ax = J.ax, &ay = J.ay;
     const int sw = J.sw, sh = J.sh, cw = J.cw, ch = J.ch;
     Guided g;
@@ -1050,15 +1068,38 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
     // and the frame's bump denominators are bounded on the host.
     const bool rcpSafe = J.bumpRcpSafe && (1.0f + maxAbsDL * maxAbsDL * invSigma2) < kRcpFastLimit;
     const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
-    if (fast && ax.sup == 8)
-        tapsSeparable<8>(c, tx0, ty0, wxp, wyp, ax.amBits ? __ldg(ax.amBits + ox) : maskBits(amx, 8),
-                         ay.amBits ? __ldg(ay.amBits + oy) : maskBits(amy, 8), a);
-    else if (fast && ax.sup == 6)
-        tapsSeparable<6>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6), a);
-    else if (fast && ax.sup == 4)
-        tapsSeparable<4>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4), a);
-    else
+    if (fast && win) {
+        // the warp staged rows ty0 .. ty0 + sup - 1 around every pixel's columns
+        const float *l0 = win->lc + (tx0 - win->tx0);
+        const double2 *u0 = win->uv + (tx0 - win->tx0);
+        if (ax.sup == 8)
+            tapsSeparable<8, true>(c, tx0, ty0, wxp, wyp,
+                                   ax.amBits ? __ldg(ax.amBits + ox) : maskBits(amx, 8),
+                                   ay.amBits ? __ldg(ay.amBits + oy) : maskBits(amy, 8),
+                                   l0, u0, kStageCols, a);
+        else if (ax.sup == 6)
+            tapsSeparable<6, true>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6),
+                                   l0, u0, kStageCols, a);
+        else
+            tapsSeparable<4, true>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4),
+                                   l0, u0, kStageCols, a);
+    } else if (fast && ax.sup <= 8 && !(ax.sup & 1) && ax.sup >= 4) {
+        const float *l0 = c.lc + (size_t)ty0 * c.cw + tx0;
+        const double2 *u0 = c.uv + (size_t)ty0 * c.cw + tx0;
+        if (ax.sup == 8)
+            tapsSeparable<8, false>(c, tx0, ty0, wxp, wyp,
+                                    ax.amBits ? __ldg(ax.amBits + ox) : maskBits(amx, 8),
+                                    ay.amBits ? __ldg(ay.amBits + oy) : maskBits(amy, 8),
+                                    l0, u0, c.cw, a);
+        else if (ax.sup == 6)
+            tapsSeparable<6, false>(c, tx0, ty0, wxp, wyp, maskBits(amx, 6), maskBits(amy, 6),
+                                    l0, u0, c.cw, a);
+        else
+            tapsSeparable<4, false>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4),
+                                    l0, u0, c.cw, a);
+    } else {
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
+    }
     if (J.tnbCount > 0) {
         // TRecon: the neighbours' motion-compensated samples follow the
         // spatial taps in the same accumulators and extend the hull
@@ -1092,8 +1133,9 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy)
 }
 
 // One listed pixel: algo 2 output, or the algo 4 selector (recon.cpp:762-811).
-__device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy) {
-    const Guided g = guidedPixel(J, ox, oy);
+__device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
+                                           const StagedWindow *win) {
+    const Guided g = guidedPixel(J, ox, oy, win);
     if (J.algo == 2) {
         emit(J, ox, oy, (float)g.u, (float)g.v);
         return;
@@ -1152,12 +1194,26 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy) {
 
 // Persistent grid over the work lists of all frames in the launch. Each
 // block builds the prefix of the frames' list lengths in shared memory and
-// strides over the concatenated work.
+// strides over the concatenated work, a warp taking 32 consecutive entries.
+//
+// STAGED: when a warp's 32 pixels are one frame's separable, unclamped fast
+// taps and share their chroma rows (one output row, as the raster-ordered
+// lists mostly give) with at most kStageCols columns between the first and
+// last window, the warp first copies that window of lc and (u, v) into its
+// shared-memory slice; the taps then read shared memory. The values and the
+// arithmetic are the same either way.
 constexpr int kGuidedMaxFrames = 1024;
+static_assert(kGuidedStageBytes == size_t(8) * kStageRows * kStageCols * (4 + 16),
+              "staged guided windows: 8 warps x kStageRows x kStageCols x (lc + (u, v))");
 
-template <int MIN_BLOCKS>
+template <int MIN_BLOCKS, bool STAGED>
 __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, int njobs) {
     __shared__ unsigned long long pre[kGuidedMaxFrames + 1];
+    extern __shared__ __align__(16) unsigned char guidedStage[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2 *sUv = reinterpret_cast<double2 *>(guidedStage) + warp * (kStageRows * kStageCols);
+    float *sLc = reinterpret_cast<float *>(guidedStage + size_t(8) * kStageRows * kStageCols * 16) +
+                 warp * (kStageRows * kStageCols);
     for (int chunk = 0; chunk < njobs; chunk += kGuidedMaxFrames) {
         const int n = min(kGuidedMaxFrames, njobs - chunk);
         if (threadIdx.x == 0) {
@@ -1172,33 +1228,87 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
         }
         __syncthreads();
         const unsigned long long total = pre[n];
-        for (unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
-             w += (unsigned long long)gridDim.x * blockDim.x) {
-            int lo = 0, hi = n - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (pre[mid] <= w) lo = mid; else hi = mid - 1;
+        const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+        for (unsigned long long wb = (unsigned long long)blockIdx.x * blockDim.x + warp * 32;
+             wb < total; wb += stride) {
+            const unsigned long long w = wb + lane;
+            const bool valid = w < total;
+            int lo = 0;
+            if (valid) {
+                int hi = n - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (pre[mid] <= w) lo = mid; else hi = mid - 1;
+                }
             }
             const FrameJob &J = jobs[chunk + lo];
-            const uint32_t pix = J.actList[w - pre[lo]];
-            guidedWork(J, (int)(pix & 0xffffu), (int)(pix >> 16));
+            const uint32_t pix = valid ? J.actList[w - pre[lo]] : 0u;
+            const int ox = (int)(pix & 0xffffu), oy = (int)(pix >> 16);
+            StagedWindow sw;
+            const StagedWindow *win = nullptr;
+            if (STAGED) {
+                const bool all = __all_sync(0xffffffffu, valid);
+                const int loMin = __reduce_min_sync(0xffffffffu, lo);
+                const int loMax = __reduce_max_sync(0xffffffffu, lo);
+                const int sup = J.ax.sup;
+                bool ok = all && loMin == loMax && !J.radial && J.noClampX && J.noClampY &&
+                          sup == J.ay.sup && sup <= kStageRows && sup >= 4 && !(sup & 1);
+                int tx0 = 0, ty0 = 0, txMin = 0, txMax = 0, tyMin = 0, tyMax = 0;
+                if (ok) {                                   // warp-uniform
+                    tx0 = __ldg(J.ax.start + ox);
+                    ty0 = __ldg(J.ay.start + oy);
+                    txMin = __reduce_min_sync(0xffffffffu, tx0);
+                    txMax = __reduce_max_sync(0xffffffffu, tx0);
+                    tyMin = __reduce_min_sync(0xffffffffu, ty0);
+                    tyMax = __reduce_max_sync(0xffffffffu, ty0);
+                    ok = tyMin == tyMax && txMax + sup - txMin <= kStageCols;
+                }
+                if (ok) {
+                    // every index in range: starts lie in [0, n - sup] (noClamp)
+                    const int cols = txMax + sup - txMin;
+                    const double2 *uvd = reinterpret_cast<const double2 *>(J.uvd);
+                    for (int k = lane; k < sup * cols; k += 32) {
+                        const int r = k / cols, cc = k - r * cols;
+                        const size_t g = (size_t)(tyMin + r) * J.cw + txMin + cc;
+                        sLc[r * kStageCols + cc] = ldf(J.lc + g);
+                        sUv[r * kStageCols + cc] = __ldg(uvd + g);
+                    }
+                    __syncwarp();
+                    sw.lc = sLc;
+                    sw.uv = sUv;
+                    sw.tx0 = txMin;
+                    sw.ty0 = tyMin;
+                    win = &sw;
+                }
+            }
+            if (valid)
+                guidedWork(J, ox, oy, win);
+            if (STAGED)
+                __syncwarp();                       // the slice is rewritten next round
         }
         __syncthreads();
     }
 }
 
-// Two register budgets of the same persistent kernel: 2 resident blocks per
-// SM (no spills) or 3 (fewer registers, a few spills); the autotuner picks.
+// Register budgets of the same persistent kernel: 2 resident blocks per SM
+// (no spills) or 3 (fewer registers, a few spills), and 2 blocks with the
+// warps' tap windows staged in shared memory; the autotuner picks.
 __global__ void __launch_bounds__(256, 2)
 k_guided(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
-    guidedGrid<2>(jobs, njobs);
+    guidedGrid<2, false>(jobs, njobs);
 }
 
 __global__ void __launch_bounds__(256, 3)
 k_guided3(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
-    guidedGrid<3>(jobs, njobs);
+    guidedGrid<3, false>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 2)
+k_guided_staged(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2, true>(jobs, njobs);
 }
 
 // Float output planes -> typed output (output conversion stage).

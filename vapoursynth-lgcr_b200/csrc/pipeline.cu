@@ -849,22 +849,23 @@ void setStageShape(int s, int bx, int by) {
     gShapeX[s] = bx; gShapeY[s] = by;
 }
 
-// Register-budget variant of the persistent guided kernel (0: 2 blocks/SM,
-// 1: 3 blocks/SM). LGCR_GUIDED_VARIANT sets the initial choice.
+// Variant of the persistent guided kernel (0: 2 blocks/SM, 1: 3 blocks/SM,
+// 2: 2 blocks/SM with the warps' tap windows staged in shared memory).
+// LGCR_GUIDED_VARIANT sets the initial choice.
 static int gGuidedVariant = -1;
 
 int guidedVariant() {
     std::lock_guard<std::mutex> lock(gShapeMu);
     if (gGuidedVariant < 0) {
         const char *e = std::getenv("LGCR_GUIDED_VARIANT");
-        gGuidedVariant = (e && e[0] == '1') ? 1 : 0;
+        gGuidedVariant = (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 0;
     }
     return gGuidedVariant;
 }
 
 void setGuidedVariant(int v) {
     std::lock_guard<std::mutex> lock(gShapeMu);
-    gGuidedVariant = v ? 1 : 0;
+    gGuidedVariant = (v >= 0 && v <= 2) ? v : 0;
 }
 
 static int stageTilesShaped(const FrameJob &J, int s);
@@ -993,16 +994,23 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     if (plan.totals[S_GUIDED] > 0) {
         // persistent grid: enough resident blocks to fill every SM
         const int variant = guidedVariant();
-        static int gridBlocks[2] = {0, 0};
+        static int gridBlocks[3] = {0, 0, 0};
+        const size_t dyn = variant == 2 ? kGuidedStageBytes : 0;
         if (gridBlocks[variant] == 0) {
             int dev = 0, sms = 0, perSm = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, variant ? k_guided3 : k_guided, 256, 0);
+            if (variant == 2)
+                cudaFuncSetAttribute(k_guided_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(kGuidedStageBytes));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &perSm, variant == 1 ? k_guided3 : variant == 2 ? k_guided_staged : k_guided, 256, dyn);
             gridBlocks[variant] = std::max(1, sms * std::max(1, perSm));
         }
-        if (variant)
+        if (variant == 1)
             k_guided3<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
+        else if (variant == 2)
+            k_guided_staged<<<gridBlocks[variant], 256, dyn, stream>>>(dJobs, pre(S_GUIDED), n);
         else
             k_guided<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
         ++launches;
