@@ -1203,6 +1203,20 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
 // shared-memory slice; the taps then read shared memory. The values and the
 // arithmetic are the same either way.
 constexpr int kGuidedMaxFrames = 1024;
+
+// cp.async copies of 4 and 16 bytes (both addresses aligned to the size)
+__device__ __forceinline__ void cpAsync4(void *smem, const void *gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpAsync16(void *smem, const void *gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" :: "r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpAsyncWaitAll() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 static_assert(kGuidedStageBytes == size_t(8) * kStageRows * kStageCols * (4 + 16),
               "staged guided windows: 8 warps x kStageRows x kStageCols x (lc + (u, v))");
 
@@ -1267,12 +1281,15 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
                     // every index in range: starts lie in [0, n - sup] (noClamp)
                     const int cols = txMax + sup - txMin;
                     const double2 *uvd = reinterpret_cast<const double2 *>(J.uvd);
+                    // asynchronous global -> shared copies (no register round
+                    // trip); the warp waits for its own copies, then syncs
                     for (int k = lane; k < sup * cols; k += 32) {
                         const int r = k / cols, cc = k - r * cols;
                         const size_t g = (size_t)(tyMin + r) * J.cw + txMin + cc;
-                        sLc[r * kStageCols + cc] = ldf(J.lc + g);
-                        sUv[r * kStageCols + cc] = __ldg(uvd + g);
+                        cpAsync4(sLc + r * kStageCols + cc, J.lc + g);
+                        cpAsync16(sUv + r * kStageCols + cc, uvd + g);
                     }
+                    cpAsyncWaitAll();
                     __syncwarp();
                     sw.lc = sLc;
                     sw.uv = sUv;
