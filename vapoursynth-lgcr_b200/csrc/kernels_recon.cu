@@ -1200,8 +1200,9 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
 // taps and share their chroma rows (one output row, as the raster-ordered
 // lists mostly give) with at most kStageCols columns between the first and
 // last window, the warp first copies that window of lc and (u, v) into its
-// shared-memory slice; the taps then read shared memory. The values and the
-// arithmetic are the same either way.
+// shared-memory slice with cp.async (global -> shared, no register round
+// trip); the taps then read shared memory. The values and the arithmetic
+// are the same either way.
 constexpr int kGuidedMaxFrames = 1024;
 
 // cp.async copies of 4 and 16 bytes (both addresses aligned to the size)
