@@ -213,6 +213,49 @@ def run_cpu(frames, specs, steps, warmup, threads, per_step, min_seconds=0.0):
     return sum(pixels) / total_s / 1e6, total_s, times
 
 
+def reference_scene_420ps(width=1920, height=1080):
+    """The reference benchmark's own source (test/benchmark.py:131-168): a
+    vertical edge, a diagonal and a low-amplitude texture in float 4:4:4,
+    here box-averaged 2x2 to 4:2:0 (the reference converts with
+    resize.Bilinear; the scene's structure, and so its sparse-active share,
+    is the same)."""
+    import numpy as np
+    yy, xx = np.mgrid[0:height, 0:width]
+    edge = (xx > width // 2).astype(np.float32)
+    diagonal = (xx * height > yy * width).astype(np.float32)
+    texture = (0.01 * np.sin(xx * 0.071) * np.cos(yy * 0.053)).astype(np.float32)
+    y = (0.2 + 0.25 * edge + 0.03 * diagonal + texture).astype(np.float32)
+    u = (-0.25 + 0.55 * edge + 0.5 * texture).astype(np.float32)
+    v = (0.30 - 0.60 * edge - 0.5 * texture).astype(np.float32)
+    box = lambda p: (0.25 * (p[0::2, 0::2] + p[1::2, 0::2] + p[0::2, 1::2] + p[1::2, 1::2])).astype(np.float32)
+    return y, box(u), box(v)
+
+
+def reference_scene_fps(seconds=3.0):
+    """Single-thread time per frame of the reference's AVX2 build on its own
+    benchmark scene at 1080p, algo 2, lanczos3, sparse, beside the published
+    figures (Ryzen 9 5950X): ties this harness to the reference's numbers."""
+    from oracle import oracle as O
+    if not O.available("avx2"):
+        return None
+    planes = reference_scene_420ps()
+    f = O.Recon(O.make_format(planes), "avx2", algo=2, kernel="lanczos", taps=3, sparse=1)
+    f.frame(planes)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        f.frame(planes)
+        n += 1
+    fps = n / (time.perf_counter() - t0)
+    _, st = f.frame(planes)
+    return {"ms_per_frame_1_thread": round(1000.0 / fps, 2),
+            "published_ms_per_frame_1_thread": 89.8,
+            "published_source": "test/baselines/lgcr-cpu-optimized-1080p.jsonl (latency mode); "
+                                "25.2 fps in the 1-thread throughput run, RELEASE_NOTES.md:19-28",
+            "sparse_active_ratio": round(st.sparse_active_ratio, 4), "published_sparse_active": 0.058,
+            "published_cpu": "AMD Ryzen 9 5950X", "scene": "1920x1080 YUV420PS edge/diagonal/texture",
+            "args": "algo 2, lanczos taps=3, sparse=1", "build": "reference AVX2 (oracle/_ref)"}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -1019,7 +1062,8 @@ def our_arm(args):
             "value": round(value_cpu, 3), "unit": "Mpix/s", "cores": threads, "kind": "reference",
             "sample": f"{len(times)} rounds of {threads} frames (alternating 1080p/4K, algo 2/6, "
                       f"one frame per thread) from the workload, reference AVX2 build "
-                      f"(oracle/_ref), {total_s:.1f} s"}
+                      f"(oracle/_ref), {total_s:.1f} s",
+            "reference_scene": reference_scene_fps()}
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
