@@ -256,6 +256,51 @@ def reference_scene_fps(seconds=3.0):
             "args": "algo 2, lanczos taps=3, sparse=1", "build": "reference AVX2 (oracle/_ref)"}
 
 
+# published 1-thread latency-mode ms per frame of the reference (Ryzen 9
+# 5950X, test/baselines/lgcr-cpu-optimized-{1080p,4k}.jsonl)
+PUBLISHED_SCENE_MS = {(1920, 1080): {2: 89.8, 4: 102.3, 6: 117.4},
+                      (3840, 2160): {2: 229.5, 4: 271.7, 6: 367.4}}
+
+
+def reference_scene_leg(dev, stream, frames=10):
+    """The reference's own benchmark scene at 1080p and 4K, algo 2/4/6,
+    lanczos3, sparse: device-path and host-path (per-frame C ABI, host
+    planes, one caller) milliseconds per frame beside the reference's
+    published single-thread figures."""
+    import numpy as np
+    import torch
+    out = {}
+    for (w, h), published in PUBLISHED_SCENE_MS.items():
+        planes = reference_scene_420ps(w, h)
+        dplanes = [torch.from_numpy(p).to(dev) for p in planes]
+        for algo, ref_ms in published.items():
+            f = lgcr.Recon(lgcr.format_of(planes), algo=algo, kernel="lanczos", taps=3, sparse=1)
+            douts = [None] + [torch.empty((h, w), dtype=torch.float32, device=dev) for _ in range(2)]
+            for _ in range(3):
+                f.frame(dplanes, -1, out=douts, stream=stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(frames):
+                f.frame(dplanes, -1, out=douts, stream=stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            dev_ms = a.elapsed_time(b) / frames
+            hout = [None] + [np.empty((h, w), np.float32) for _ in range(2)]
+            f.frame(planes, -1, out=hout)
+            lat = []
+            for _ in range(frames):
+                t0 = time.perf_counter()
+                f.frame(planes, -1, out=hout)
+                lat.append(1000 * (time.perf_counter() - t0))
+            out[f"{w}x{h} algo{algo}"] = {"device_ms": round(dev_ms, 3),
+                                          "host_call_ms": round(statistics.median(lat), 3),
+                                          "reference_published_ms": ref_ms}
+            f.close()
+    return {"scene": "the reference's benchmark scene (edge/diagonal/texture), YUV420PS, "
+                     "lanczos taps=3, sparse=1", "frames": out}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -1047,6 +1092,7 @@ def our_arm(args):
 
     if clip is not None:
         result["filters"] = filters_leg(clip, dev, stream, max(3, min(args.steps, 10)), args.warmup)
+        result["reference_scene"] = reference_scene_leg(dev, stream)
 
     if rank == 0 and args.serve_requests > 0:
         # content of the serving stream (spawned workers: safe after CUDA init)
