@@ -63,7 +63,8 @@ def test_batched_and_graph_replay_vs_oracle():
     refs = [refs[:4], refs[4:]]
     batch = ctypes.c_void_p()
     assert lib.lgcr_batch_create(ctypes.byref(batch)) == 0
-    stream = torch.cuda.current_stream().cuda_stream
+    side = torch.cuda.Stream()                 # graphs are captured on a created stream
+    stream = side.cuda_stream
     try:
         # (frame set, use_graph): direct launches, graph capture, graph replay
         # with new frames in the same layout, direct again
@@ -77,6 +78,7 @@ def test_batched_and_graph_replay_vs_oracle():
                 items[i].inp = lgcr.planes_desc(dins[i])
                 items[i].out = lgcr.planes_desc(douts[i])
                 items[i].chroma_location = -1
+            side.wait_stream(torch.cuda.current_stream())
             st = lib.lgcr_batch_run(batch, items, len(LAYOUT), ctypes.c_void_p(stream), use_graph)
             assert st == 0, lib.lgcr_last_error().decode()
             torch.cuda.synchronize()
@@ -84,6 +86,32 @@ def test_batched_and_graph_replay_vs_oracle():
             for i, (w, h, a) in enumerate(LAYOUT):
                 assert_parity(to_host(douts[i]), refs[which][i], False,
                               f"batched set {which} graph={use_graph} {w}x{h} algo {a}")
+    finally:
+        lib.lgcr_batch_destroy(batch)
+
+
+def test_graph_request_on_the_default_stream_runs_directly():
+    """The legacy default stream cannot be captured: a graph request there
+    launches the stages directly, with the same results."""
+    lib = lgcr.library()
+    rec = lgcr.Recon(lgcr.video_format(320, 180, 10, 1, 1), algo=2, **BATCH_ARGS)
+    planes = S.make_frame(320, 180, S.YUV420P10, seed=77)
+    ref = oracle_frames([(planes, 10, dict(algo=2, **BATCH_ARGS))])[0]
+    dins = to_device(planes)
+    douts = [torch.empty((180, 320), dtype=torch.int16, device="cuda").view(torch.uint16)
+             for _ in range(3)]
+    items = (lgcr.BatchItem * 1)()
+    items[0].filter = rec.handle
+    items[0].inp = lgcr.planes_desc(dins)
+    items[0].out = lgcr.planes_desc(douts)
+    items[0].chroma_location = -1
+    batch = ctypes.c_void_p()
+    assert lib.lgcr_batch_create(ctypes.byref(batch)) == 0
+    try:
+        torch.cuda.synchronize()
+        assert lib.lgcr_batch_run(batch, items, 1, None, 1) == 0, lib.lgcr_last_error().decode()
+        torch.cuda.synchronize()
+        assert_parity(to_host(douts), ref, False, "default-stream graph request")
     finally:
         lib.lgcr_batch_destroy(batch)
 

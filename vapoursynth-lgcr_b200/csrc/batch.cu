@@ -237,7 +237,9 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
     std::memcpy(sl.hJobs, jobs.data(), sizeof(FrameJob) * count);
     std::memcpy(sl.hPrefix, plan.prefix.data(), plan.prefix.size() * sizeof(int));
     int launches = -1;
-    if (use_graph && !b->profiling) {
+    // the legacy default stream cannot be captured: its runs launch directly
+    const bool capturable = s != nullptr && s != cudaStreamLegacy;
+    if (use_graph && !b->profiling && capturable) {
         if (!sl.exec || sl.signature != sig) {
             if (sl.exec) { cudaGraphExecDestroy(sl.exec); sl.exec = nullptr; }
             sl.signature.clear();
