@@ -350,6 +350,8 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     c.rad = J.srad;
     c.invWxC = J.sinvWxC;
     c.invWyC = J.sinvWyC;
+    c.noClampX = J.sNoClampX;
+    c.noClampY = J.sNoClampY;
     float r, unused;
     plainAt(c, x, y, r, unused);
     J.detailTmp[o] = ldf(J.Y + o) - r;

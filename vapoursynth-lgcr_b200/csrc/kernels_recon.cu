@@ -738,14 +738,20 @@ __device__ __forceinline__ void accumulate(Acc &a, float w, double2 p) {
 // lc0/uv0 point at the window's tap (0, 0); rows are `stride` samples apart.
 // SH: the window was staged in shared memory by the warp (plain loads);
 // otherwise it is read from the planes in global memory.
-template <int SUP, bool SH>
+// RADIAL: the base weight of tap (i, j) is the radial table's entry rad[j *
+// SUP + i] (the jinc phase table of the output pixel) instead of wx(i) * wy(j).
+template <int SUP, bool SH, bool RADIAL = false>
 __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0, const float *wxp,
                                               const float *wyp, uint32_t mx, uint32_t my,
                                               const float *lc0, const double2 *uv0, int stride,
-                                              Acc &a) {
+                                              Acc &a, const float *rad = nullptr) {
     constexpr int NP = SUP / 2;
     f32x2 dxnx[NP], dxny[NP], wxv[NP];
-    if (SUP % 4 == 0) {
+    if (RADIAL) {
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
+            wxv[q] = 0ull;
+    } else if (SUP % 4 == 0) {
         // the column's weights as 16-byte loads (rows of SUP floats in a
         // 256-byte aligned table)
 #pragma unroll
@@ -776,9 +782,10 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
             continue;
         const float *lrow = lc0 + (size_t)j * stride;
         const double2 *uvrow = uv0 + (size_t)j * stride;
-        const float wy = __ldg(wyp + j);
+        const float wy = RADIAL ? 0.0f : __ldg(wyp + j);
         const float dy = ((float)(ty0 + j) - c.scy) * c.rhF;
         const f32x2 wyy = pk2(wy, wy);
+        const float2 *radRow = RADIAL ? reinterpret_cast<const float2 *>(rad + j * SUP) : nullptr;
         const f32x2 dyny = pk2(dy * c.ny, dy * c.ny), dynx = pk2(dy * c.nx, dy * c.nx);
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
@@ -792,7 +799,14 @@ __device__ __forceinline__ void tapsSeparable(const TapCtx &c, int tx0, int ty0,
             const f32x2 dp = add2(dxnx[q], dyny);
             const f32x2 dt = add2(dxny[q], dynx);
             const f32x2 bump = rcp2(add2(add2(one, mul2(mul2(dp, dp), g2)), mul2(mul2(dt, dt), g2p)), one);
-            const f32x2 w = mul2(sim, add2(mul2(wxv[q], wyy), mul2(resc, bump)));
+            f32x2 base;
+            if (RADIAL) {
+                const float2 r2 = __ldg(radRow + q);
+                base = pk2(r2.x, r2.y);
+            } else {
+                base = mul2(wxv[q], wyy);
+            }
+            const f32x2 w = mul2(sim, add2(base, mul2(resc, bump)));
             float w0, w1;
             up2(w, w0, w1);
             if ((mx >> i) & 1u)
@@ -1068,6 +1082,10 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     // and the frame's bump denominators are bounded on the host.
     const bool rcpSafe = J.bumpRcpSafe && (1.0f + maxAbsDL * maxAbsDL * invSigma2) < kRcpFastLimit;
     const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
+    // jinc with a phase table: the same unrolled loop with table weights
+    const bool fastRadial = J.radial && J.rad.valid && J.rad.supX == ax.sup && J.rad.supY == ay.sup &&
+                            J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe &&
+                            (ax.sup == 4 || ax.sup == 6 || ax.sup == 8);
     if (fast && win) {
         // the warp staged rows ty0 .. ty0 + sup - 1 around every pixel's columns
         const float *l0 = win->lc + (tx0 - win->tx0);
@@ -1097,6 +1115,19 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
         else
             tapsSeparable<4, false>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4),
                                     l0, u0, c.cw, a);
+    } else if (fastRadial) {
+        const float *l0 = c.lc + (size_t)ty0 * c.cw + tx0;
+        const double2 *u0 = c.uv + (size_t)ty0 * c.cw + tx0;
+        const float *rad = radialWeightsAt(J.rad, ox, oy);
+        if (ax.sup == 6)
+            tapsSeparable<6, false, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 6),
+                                          maskBits(amy, 6), l0, u0, c.cw, a, rad);
+        else if (ax.sup == 8)
+            tapsSeparable<8, false, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 8),
+                                          maskBits(amy, 8), l0, u0, c.cw, a, rad);
+        else
+            tapsSeparable<4, false, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 4),
+                                          maskBits(amy, 4), l0, u0, c.cw, a, rad);
     } else {
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
     }
@@ -1385,11 +1416,14 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
 
 // 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x8
 // block of output pixels stages the clamped input rows and columns its
-// windows cover and the kernel's LUT in shared memory (when they fit), so
-// the sup x sup taps read shared memory; the tap weights and the FP64
-// accumulation follow the reference's order and arithmetic.
-constexpr int kRadialTileMax = 6144;         // staged luma samples per block
+// windows cover (as doubles, the accumulation's operand type) and the
+// kernel's LUT in shared memory when they fit, so the sup x sup taps read
+// shared memory; each pixel's column offsets are converted once, not once per
+// row. The tap weights and the FP64 accumulation follow the reference's
+// order and arithmetic.
+constexpr int kRadialTileMax = 3072;         // staged luma samples per block
 constexpr int kRadialLutMax = 4096;          // staged LUT entries
+constexpr int kRadialMaxSup = 16;            // column offsets kept per pixel
 
 __device__ __forceinline__ float lutLookupShared(const float *lut, int n, float idx) {
     int i0 = (int)idx;
@@ -1401,7 +1435,7 @@ __device__ __forceinline__ float lutLookupShared(const float *lut, int n, float 
 
 __global__ void __launch_bounds__(256)
 k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
-    __shared__ float sY[kRadialTileMax];
+    __shared__ double sY[kRadialTileMax];
     __shared__ float sLut[kRadialLutMax];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
@@ -1426,8 +1460,8 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     const int nt = blockDim.x * blockDim.y, t = threadIdx.y * blockDim.x + threadIdx.x;
     if (tileStaged)
         for (int k = t; k < fw * fh; k += nt)
-            sY[k] = ldf(J.Y + (size_t)iclamp(fy0 + k / fw, 0, J.sh - 1) * J.sw +
-                        iclamp(fx0 + k % fw, 0, J.sw - 1));
+            sY[k] = (double)ldf(J.Y + (size_t)iclamp(fy0 + k / fw, 0, J.sh - 1) * J.sw +
+                                iclamp(fx0 + k % fw, 0, J.sw - 1));
     if (lutStaged)
         for (int k = t; k < J.lutN; k += nt)
             sLut[k] = ldf(J.lut + k);
@@ -1438,19 +1472,37 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     const int y0 = (int)ceil(cy - radius);
     const double cx = (ox + 0.5) * sx - 0.5;
     const int x0 = (int)ceil(cx - radius);
+    float dxs[kRadialMaxSup];
+    const bool keepDx = sup <= kRadialMaxSup;
+    if (keepDx) {
+#pragma unroll
+        for (int i = 0; i < kRadialMaxSup; ++i)
+            if (i < sup)
+                dxs[i] = (float)((x0 + i - cx) * invW);
+    }
     double acc = 0.0, wsum = 0.0;
     for (int j = 0; j < sup; ++j) {
-        const int ty = iclamp(y0 + j, 0, J.sh - 1);
         const float dy = (float)((y0 + j - cy) * invW);
-        const float *row = J.Y + (size_t)ty * J.sw;
         const int srow = (y0 + j - fy0) * fw - fx0;
+        const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
+        if (keepDx && tileStaged && lutStaged) {
+#pragma unroll
+            for (int i = 0; i < kRadialMaxSup; ++i) {
+                if (i >= sup)
+                    break;
+                const float dx = dxs[i];
+                const float w = lutLookupShared(sLut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
+                acc = fma((double)w, sY[srow + x0 + i], acc);
+                wsum += (double)w;
+            }
+            continue;
+        }
         for (int i = 0; i < sup; ++i) {
             const float dx = (float)((x0 + i - cx) * invW);
             const float r = sqrtf(dx * dx + dy * dy) * J.lutScale;
-            const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r)
-                                      : lutLookupDev(J.lut, J.lutN, r);
-            const float v = tileStaged ? sY[srow + x0 + i] : ldf(row + iclamp(x0 + i, 0, J.sw - 1));
-            acc = fma((double)w, (double)v, acc);
+            const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r) : lutLookupDev(J.lut, J.lutN, r);
+            const double v = tileStaged ? sY[srow + x0 + i] : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
+            acc = fma((double)w, v, acc);
             wsum += (double)w;
         }
     }

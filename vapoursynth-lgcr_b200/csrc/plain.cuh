@@ -19,6 +19,7 @@ struct PlainCtx {
     float margin, invWxC, invWyC, lutScale;
     int lutN;
     const float *lut;
+    int noClampX, noClampY;      // every tap index of the axes is in range
 };
 
 __device__ __forceinline__ void plainSeparableAt(const PlainCtx &c, int ox, int oy, float &o0, float &o1) {
@@ -86,6 +87,70 @@ __device__ __forceinline__ const float *radialWeightsAt(const RadialView &r, int
     return r.weights + phase * (size_t)r.supX * r.supY;
 }
 
+// Radial plain base with the phase table, taps in range and an even support
+// SUP: the loop of plainRadialAt fully unrolled, tap activity from bit
+// masks, weight pairs as 8-byte loads; the same sums in the same order.
+template <int SUP>
+__device__ __forceinline__ void plainRadialTable(const PlainCtx &c, int ox, int oy, const float *base,
+                                                 float &o0, float &o1) {
+    const AxisView &ax = c.ax, &ay = c.ay;
+    const int tx0 = __ldg(ax.start + ox), ty0 = __ldg(ay.start + oy);
+    uint32_t mx = 0, my = 0;
+#pragma unroll
+    for (int i = 0; i < SUP; ++i) {
+        mx |= (__ldg(ax.am + (size_t)ox * SUP + i) != 0 ? 1u : 0u) << i;
+        my |= (__ldg(ay.am + (size_t)oy * SUP + i) != 0 ? 1u : 0u) << i;
+    }
+    const float scx = __ldg(ax.pos + ox), scy = __ldg(ay.pos + oy);
+    const bool dual = c.p1 != nullptr;
+    double acc0 = 0.0, acc1 = 0.0, wsum = 0.0, sumAbs = 0.0;
+    float mn0 = 1e30f, mx0 = -1e30f, mn1 = 1e30f, mx1 = -1e30f;
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((my >> j) & 1u))
+            continue;
+        const float *r0 = c.p0 + (size_t)(ty0 + j) * c.w + tx0;
+        const float *r1 = dual ? c.p1 + (size_t)(ty0 + j) * c.w + tx0 : nullptr;
+        const float2 *wrow = reinterpret_cast<const float2 *>(base + j * SUP);
+#pragma unroll
+        for (int q = 0; q < SUP / 2; ++q) {
+            const float2 w2 = __ldg(wrow + q);
+            const float wk[2] = { w2.x, w2.y };
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = 2 * q + h;
+                if (!((mx >> i) & 1u))
+                    continue;
+                const float weight = wk[h];
+                const float a = ldf(r0 + i);
+                acc0 = fma((double)weight, (double)a, acc0);
+                wsum += (double)weight;
+                sumAbs += (double)fabsf(weight);
+                mn0 = smin(mn0, a); mx0 = smax(mx0, a);
+                if (dual) {
+                    const float b = ldf(r1 + i);
+                    acc1 = fma((double)weight, (double)b, acc1);
+                    mn1 = smin(mn1, b); mx1 = smax(mx1, b);
+                }
+            }
+        }
+    }
+    double v0, v1 = 0.0;
+    if (wsum > 1e-6 && wsum >= 0.05 * sumAbs) {
+        v0 = acc0 / wsum;
+        if (dual) v1 = acc1 / wsum;
+    } else {
+        v0 = bilinearAt(c.p0, c.w, c.h, scx, scy);
+        if (dual) v1 = bilinearAt(c.p1, c.w, c.h, scx, scy);
+    }
+    if (c.clampHull) {
+        v0 = sclamp(v0, (double)(mn0 - c.margin), (double)(mx0 + c.margin));
+        if (dual) v1 = sclamp(v1, (double)(mn1 - c.margin), (double)(mx1 + c.margin));
+    }
+    o0 = (float)v0;
+    o1 = (float)v1;
+}
+
 __device__ __forceinline__ void plainRadialAt(const PlainCtx &c, int ox, int oy, float &o0, float &o1) {
     const AxisView &ax = c.ax, &ay = c.ay;
     const int tx0 = __ldg(ax.start + ox), ty0 = __ldg(ay.start + oy);
@@ -93,6 +158,15 @@ __device__ __forceinline__ void plainRadialAt(const PlainCtx &c, int ox, int oy,
     const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
     const float scx = __ldg(ax.pos + ox), scy = __ldg(ay.pos + oy);
     const float *base = radialWeightsAt(c.rad, ox, oy);
+    if (base && c.noClampX && c.noClampY && ax.sup == ay.sup && c.rad.supX == ax.sup &&
+        c.rad.supY == ay.sup) {
+        switch (ax.sup) {
+        case 4: plainRadialTable<4>(c, ox, oy, base, o0, o1); return;
+        case 6: plainRadialTable<6>(c, ox, oy, base, o0, o1); return;
+        case 8: plainRadialTable<8>(c, ox, oy, base, o0, o1); return;
+        default: break;
+        }
+    }
     const bool dual = c.p1 != nullptr;
     double acc0 = 0.0, acc1 = 0.0, wsum = 0.0, sumAbs = 0.0;
     float mn0 = 1e30f, mx0 = -1e30f, mn1 = 1e30f, mx1 = -1e30f;
@@ -161,6 +235,7 @@ __device__ __forceinline__ PlainCtx chromaPlainCtx(const FrameJob &J) {
     c.kernel = J.kernel; c.radial = J.radial; c.clampHull = J.clampHull;
     c.margin = J.margin; c.invWxC = J.invWxC; c.invWyC = J.invWyC;
     c.lutScale = J.lutScale; c.lutN = J.lutN; c.lut = J.lut;
+    c.noClampX = J.noClampX; c.noClampY = J.noClampY;
     return c;
 }
 
