@@ -363,7 +363,8 @@ def serve_requests(n, seed=4000):
 
 
 def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30,
-                sweep_factors=(0.5, 0.8, 1.0, 1.5), sweep_requests=600):
+                sweep_factors=(0.5, 0.7, 0.9, 1.1), sweep_requests=600,
+                sweep_servers=((2, 8), (2, 4), (3, 2))):
     """Poisson arrivals at 1.2x the per-frame path's capacity into the
     continuous-batching server, then shorter streams at other rates; latency
     from submit to completion on the server's clock."""
@@ -415,11 +416,11 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30,
         filt(k, algo, bm).frame(pins[(k, s % SERVE_SEEDS)], -1, out=out_set(k)[1])
     plain_fps = len(sample) / (time.perf_counter() - t0)
 
-    def run_stream(stream_reqs, rate, seed):
+    def run_stream(stream_reqs, rate, seed, n_lanes=lanes, batch_cap=max_batch):
         """Poisson arrivals at `rate` frames/s; per-request latency from submit
         to completion on the server's clock."""
         arrivals = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, len(stream_reqs)))
-        server = lgcr.Server(budget_bytes=budget, max_batch=max_batch, lanes=lanes,
+        server = lgcr.Server(budget_bytes=budget, max_batch=batch_cap, lanes=n_lanes,
                              queue_capacity=len(stream_reqs) + 1)
         tickets = [None] * len(stream_reqs)
         owner = {}                     # (kind, ring slot) -> request index using it
@@ -459,10 +460,12 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30,
     # arrival-rate sweep: the highest rate whose p99 stays under 100 ms is the
     # sustainable throughput of this mixed stream
     sweep = []
-    for factor in sweep_factors:
-        r = run_stream(reqs[:sweep_requests], factor * plain_fps, 4100 + int(100 * factor))
-        r["rate_factor"] = factor
-        sweep.append(r)
+    for (n_lanes, batch_cap) in sweep_servers:
+        for factor in sweep_factors:
+            r = run_stream(reqs[:sweep_requests], factor * plain_fps, 4100 + int(100 * factor),
+                           n_lanes, batch_cap)
+            r.update(rate_factor=factor, lanes=n_lanes, max_batch=batch_cap)
+            sweep.append(r)
     ok = [r for r in sweep if r["latency_ms"]["p99"] <= 100.0 and r["failed"] == 0]
     best = max(ok, key=lambda r: r["throughput_mpix_s"]) if ok else None
     return dict(main, **{
@@ -474,6 +477,7 @@ def serving_leg(frames, n_requests, lanes=2, max_batch=8, budget=8 << 30,
         "sweep": sweep,
         "sustainable_p99_under_100ms": ({"arrival_rate_fps": best["arrival_rate_fps"],
                                          "throughput_mpix_s": best["throughput_mpix_s"],
+                                         "lanes": best["lanes"], "max_batch": best["max_batch"],
                                          "latency_ms": best["latency_ms"]} if best else None)})
 
 
