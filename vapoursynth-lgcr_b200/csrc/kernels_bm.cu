@@ -73,6 +73,8 @@ k_bm_group(LGCR_STAGE_ARGS) {
     __shared__ float costs[8][32];
     __shared__ int cbx[8][32], cby[8][32];
     __shared__ int meta[8][kAnchorInts];
+    __shared__ float bestC[8][kGroup];
+    __shared__ int bestX[8][kGroup], bestY[8][kGroup];
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -107,46 +109,54 @@ k_bm_group(LGCR_STAGE_ARGS) {
         costs[warp][lane] = cost;
     }
     __syncwarp();
-    if (lane == 0) {
-        // dedup in enumeration order + insertion into the best-4 list
-        float mc[kGroup];
-        int mx[kGroup], my[kGroup];
-        int count = 0, seen = 0;
-        int sx[25], sy[25];
-        for (int c = 0; c < 25; ++c) {
-            const int bx = cbx[warp][c], by = cby[warp][c];
-            bool dup = false;
-            for (int i = 0; i < seen; ++i)
-                if (sx[i] == bx && sy[i] == by) { dup = true; break; }
-            if (dup)
-                continue;
-            sx[seen] = bx; sy[seen] = by; ++seen;
-            const float cost = costs[warp][c];
-            int position = min(count, kGroup - 1);
-            if (count == kGroup && cost >= mc[kGroup - 1])
-                continue;
-            if (count < kGroup)
-                ++count;
-            while (position > 0 && cost < mc[position - 1]) {
-                if (position < kGroup) {
-                    mc[position] = mc[position - 1];
-                    mx[position] = mx[position - 1];
-                    my[position] = my[position - 1];
-                }
-                --position;
+    // The reference walks the candidates in enumeration order, skips a
+    // position seen before and inserts the rest into a best-4 list that keeps
+    // an earlier candidate ahead of a later one of equal cost: the list holds
+    // the 4 smallest kept candidates by (cost, enumeration index). Each lane
+    // finds whether its candidate is kept and its rank among the kept ones.
+    bool keep = false;
+    float myCost = 0.0f;
+    int myBx = 0, myBy = 0;
+    if (lane < 25) {
+        myBx = cbx[warp][lane];
+        myBy = cby[warp][lane];
+        myCost = costs[warp][lane];
+        keep = true;
+        for (int i = 0; i < lane; ++i)
+            if (cbx[warp][i] == myBx && cby[warp][i] == myBy) {
+                keep = false;
+                break;
             }
-            mc[position] = cost; mx[position] = bx; my[position] = by;
+    }
+    const unsigned kept = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+        int rank = 0;
+        for (int d = 0; d < 25; ++d) {
+            if (d == lane || !((kept >> d) & 1u))
+                continue;
+            const float cd = costs[warp][d];
+            if (cd < myCost || (cd == myCost && d < lane))
+                ++rank;
         }
+        if (rank < kGroup) {
+            bestC[warp][rank] = myCost;
+            bestX[warp][rank] = myBx;
+            bestY[warp][rank] = myBy;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        const int count = min(__popc(kept), kGroup);
         const float gs = J.bmSigma;
         const float matchLimit = smax(4e-5f, 4.0f * gs * gs);
         int eligible = 0;
-        while (eligible < count && mc[eligible] <= matchLimit)
+        while (eligible < count && bestC[warp][eligible] <= matchLimit)
             ++eligible;
         const int groupCount = eligible >= 4 ? 4 : (eligible >= 2 ? 2 : 1);
         meta[warp][0] = groupCount < 2 ? 0 : groupCount;
         for (int k = 0; k < kGroup; ++k) {
-            meta[warp][1 + 2 * k] = k < count ? mx[k] : 0;
-            meta[warp][2 + 2 * k] = k < count ? my[k] : 0;
+            meta[warp][1 + 2 * k] = k < count ? bestX[warp][k] : 0;
+            meta[warp][2 + 2 * k] = k < count ? bestY[warp][k] : 0;
         }
     }
     __syncwarp();
