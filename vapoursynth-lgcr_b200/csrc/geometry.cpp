@@ -236,6 +236,7 @@ RadialTable buildRadialTable(const KernelSpec &k, const ChromaAxis &ax, const Ch
     t.weights.assign(phasePairs * perPhase, 0.0f);
     t.weightSum.resize(phasePairs);
     t.absoluteWeightSum.resize(phasePairs);
+    t.kappa.resize(phasePairs);
     const float invX = float(std::min(1.0, double(ax.n) / sourceWidth));
     const float invY = float(std::min(1.0, double(ay.n) / sourceHeight));
     const int lutN = int(k.lut.size());
@@ -260,6 +261,17 @@ RadialTable buildRadialTable(const KernelSpec &k, const ChromaAxis &ax, const Ch
             }
             t.weightSum[phase] = sum;
             t.absoluteWeightSum[phase] = absSum;
+            float m = 0.0f, q = 0.0f;
+            for (int j = 0; j < ay.sup; ++j)
+                for (int i = 0; i < ax.sup; ++i) {
+                    if ((xActivity[px] & (uint64_t{1} << i)) == 0 ||
+                        (yActivity[py] & (uint64_t{1} << j)) == 0)
+                        continue;
+                    const float wv = w[size_t(j) * ax.sup + i];
+                    m = (m < std::fabs(wv)) ? std::fabs(wv) : m;
+                    q += wv * wv;
+                }
+            t.kappa[phase] = (m * m) / (q + 1e-12f);
         }
     return t;
 }

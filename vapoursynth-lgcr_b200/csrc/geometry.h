@@ -69,6 +69,9 @@ struct RadialTable {
     std::vector<uint16_t> xPhase, yPhase;
     std::vector<float> weights;
     std::vector<double> weightSum, absoluteWeightSum;
+    // per phase pair: the guided rescue's kappa (max |w|)^2 / (sum w^2 + 1e-12)
+    // over the active taps, in float and in tap order (rows, then columns)
+    std::vector<float> kappa;
 };
 
 RadialTable buildRadialTable(const KernelSpec &k, const ChromaAxis &ax, const ChromaAxis &ay,

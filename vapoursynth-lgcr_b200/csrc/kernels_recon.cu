@@ -875,6 +875,34 @@ __device__ __forceinline__ void windowExtrema(const FrameJob &J, int ox, int ty0
     ext[0] = mnU; ext[1] = mxU; ext[2] = mnV; ext[3] = mxV; ext[4] = mnL; ext[5] = mxL;
 }
 
+// Pass 1 of the guided pixel over a window whose taps are all in range:
+// h = {max |lc - L0|, min U, max U, min V, max V} over the active taps, in
+// the generic loop's order (rows, then columns) with bit masks and no
+// clamping.
+template <int SUP>
+__device__ __forceinline__ void windowHullInRange(const FrameJob &J, int tx0, int ty0,
+                                                  const uint8_t *amx, const uint8_t *amy, float L0,
+                                                  float *h) {
+    const uint32_t mx = maskBits(amx, SUP), my = maskBits(amy, SUP);
+    float maxAbsDL = 0.0f, mnU = 1e30f, mxU = -1e30f, mnV = 1e30f, mxV = -1e30f;
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((my >> j) & 1u))
+            continue;
+        const size_t row = (size_t)(ty0 + j) * J.cw + tx0;
+#pragma unroll
+        for (int i = 0; i < SUP; ++i) {
+            if (!((mx >> i) & 1u))
+                continue;
+            const float l = ldf(J.lc + row + i), u = ldf(J.U + row + i), v = ldf(J.V + row + i);
+            maxAbsDL = smax(maxAbsDL, fabsf(l - L0));
+            mnU = smin(mnU, u); mxU = smax(mxU, u);
+            mnV = smin(mnV, v); mxV = smax(mxV, v);
+        }
+    }
+    h[0] = maxAbsDL; h[1] = mnU; h[2] = mxU; h[3] = mnV; h[4] = mxV;
+}
+
 struct Guided {
     double u, v;
     float L0, ssRamp, guideFade, nx, ny;
@@ -976,6 +1004,15 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
         hMinU = ext[0]; hMaxU = ext[1]; hMinV = ext[2]; hMaxV = ext[3];
         maxAbsDL = smax(maxAbsDL, fabsf(ext[5] - L0));
         maxAbsDL = smax(maxAbsDL, fabsf(ext[4] - L0));
+    } else if (J.noClampX && J.noClampY && ax.sup == ay.sup &&
+               (ax.sup == 4 || ax.sup == 6 || ax.sup == 8)) {
+        float h[5];
+        switch (ax.sup) {
+        case 4: windowHullInRange<4>(J, tx0, ty0, amx, amy, L0, h); break;
+        case 6: windowHullInRange<6>(J, tx0, ty0, amx, amy, L0, h); break;
+        default: windowHullInRange<8>(J, tx0, ty0, amx, amy, L0, h); break;
+        }
+        maxAbsDL = h[0]; hMinU = h[1]; hMaxU = h[2]; hMinV = h[3]; hMaxV = h[4];
     } else {
         for (int j = 0; j < ay.sup; ++j) {
             if (__ldg(amy + j) == 0)
@@ -1043,6 +1080,12 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
                 const float mxX = __ldg(ax.kmx + ox), ssX = __ldg(ax.kss + ox);
                 const float mxY = __ldg(ay.kmx + oy), ssY = __ldg(ay.kss + oy);
                 kappa = (mxX * mxX * mxY * mxY) / (ssX * ssY + 1e-12f);
+            } else if (J.rad.valid && J.rad.kappa) {
+                // the phase table's kappa: the same float sums over the
+                // phase's active taps, evaluated once per phase on the host
+                const size_t phase = (size_t)__ldg(J.rad.yPhase + oy) * J.rad.phasesX +
+                                     __ldg(J.rad.xPhase + ox);
+                kappa = ldf(J.rad.kappa + phase);
             } else {
                 const float *base = radialWeightsAt(J.rad, ox, oy);
                 float mx = 0, ss = 0;

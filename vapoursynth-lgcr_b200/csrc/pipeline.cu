@@ -274,13 +274,14 @@ WeightView weightView(const DeviceArena &ar, const WeightOffsets &o) {
     return { o.n, o.sup, (const int *)ar.at(o.start), (const float *)ar.at(o.w) };
 }
 
-struct RadialOffsets { size_t xPhase, yPhase, weights; int valid, supX, supY, phasesX; };
+struct RadialOffsets { size_t xPhase, yPhase, weights, kappa; int valid, supX, supY, phasesX; };
 RadialOffsets packRadial(Packer &pk, const RadialTable &t) {
     RadialOffsets o{};
     o.valid = t.valid;
     o.supX = t.supportX; o.supY = t.supportY; o.phasesX = t.phaseCountX;
     if (t.valid) {
         o.xPhase = pk.add(t.xPhase); o.yPhase = pk.add(t.yPhase); o.weights = pk.add(t.weights);
+        o.kappa = pk.add(t.kappa);
     }
     return o;
 }
@@ -292,6 +293,7 @@ RadialView radialView(const DeviceArena &ar, const RadialOffsets &o) {
         v.xPhase = (const uint16_t *)ar.at(o.xPhase);
         v.yPhase = (const uint16_t *)ar.at(o.yPhase);
         v.weights = (const float *)ar.at(o.weights);
+        v.kappa = (const float *)ar.at(o.kappa);
     }
     return v;
 }

@@ -42,6 +42,7 @@ struct RadialView {
     int supX, supY, phasesX;
     const uint16_t *xPhase, *yPhase;
     const float *weights;
+    const float *kappa;      // per phase pair: the guided rescue's kappa, or null
 };
 
 // One temporal neighbour of a TRecon frame (TemporalNbr, src/lgcr.h:729-736):
