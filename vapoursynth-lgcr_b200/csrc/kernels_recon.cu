@@ -1460,13 +1460,17 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
 // 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x8
 // block of output pixels stages the clamped input rows and columns its
 // windows cover (as doubles, the accumulation's operand type) and the
-// kernel's LUT in shared memory when they fit, so the sup x sup taps read
-// shared memory; each pixel's column offsets are converted once, not once per
-// row. The tap weights and the FP64 accumulation follow the reference's
-// order and arithmetic.
-constexpr int kRadialTileMax = 3072;         // staged luma samples per block
+// kernel's LUT in shared memory when they fit. A tap's weight depends only
+// on the pixel's column offsets (x0 + i - cx) / widen and row offsets
+// (y0 + j - cy) / widen as floats; the block groups its columns (and rows)
+// whose offset vectors are identical, evaluates the weights once per
+// (column group, row group) into a shared table of doubles, and every pixel
+// then accumulates from shared memory. The weights, their order and the FP64
+// accumulation are the reference's.
+constexpr int kRadialTileMax = 2048;         // staged luma samples per block
 constexpr int kRadialLutMax = 4096;          // staged LUT entries
-constexpr int kRadialMaxSup = 16;            // column offsets kept per pixel
+constexpr int kRadialMaxSup = 16;            // offsets kept per column / row
+constexpr int kRadialWeightsMax = 1152;      // shared weight table (doubles)
 
 __device__ __forceinline__ float lutLookupShared(const float *lut, int n, float idx) {
     int i0 = (int)idx;
@@ -1480,6 +1484,10 @@ __global__ void __launch_bounds__(256)
 k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     __shared__ double sY[kRadialTileMax];
     __shared__ float sLut[kRadialLutMax];
+    __shared__ double sW[kRadialWeightsMax];
+    __shared__ float sDx[32][kRadialMaxSup], sDy[8][kRadialMaxSup];
+    __shared__ int sColClass[32], sRowClass[8], sColIdx[32], sRowIdx[8];
+    __shared__ int sColN, sRowN;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
@@ -1500,6 +1508,7 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     const int fh = (int)ceil((byLast + 0.5) * sy - 0.5 - radius) + sup - fy0;
     const bool tileStaged = fw * fh <= kRadialTileMax;
     const bool lutStaged = J.lutN <= kRadialLutMax;
+    const bool grouped = tileStaged && lutStaged && sup <= kRadialMaxSup;
     const int nt = blockDim.x * blockDim.y, t = threadIdx.y * blockDim.x + threadIdx.x;
     if (tileStaged)
         for (int k = t; k < fw * fh; k += nt)
@@ -1508,45 +1517,108 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     if (lutStaged)
         for (int k = t; k < J.lutN; k += nt)
             sLut[k] = ldf(J.lut + k);
-    __syncthreads();
-    if (ox >= J.W || oy >= J.H)
-        return;
     const double cy = (oy + 0.5) * sy - 0.5;
     const int y0 = (int)ceil(cy - radius);
     const double cx = (ox + 0.5) * sx - 0.5;
     const int x0 = (int)ceil(cx - radius);
-    float dxs[kRadialMaxSup];
-    const bool keepDx = sup <= kRadialMaxSup;
-    if (keepDx) {
-#pragma unroll
-        for (int i = 0; i < kRadialMaxSup; ++i)
-            if (i < sup)
-                dxs[i] = (float)((x0 + i - cx) * invW);
+    bool tabled = false;
+    if (grouped) {
+        // offset vectors of the block's columns (row 0 of threads) and rows
+        // (column 0 of threads), then each one's first identical predecessor
+        if (threadIdx.y == 0)
+            for (int i = 0; i < sup; ++i)
+                sDx[threadIdx.x][i] = (float)((x0 + i - cx) * invW);
+        if (threadIdx.x == 0)
+            for (int j = 0; j < sup; ++j)
+                sDy[threadIdx.y][j] = (float)((y0 + j - cy) * invW);
+        __syncthreads();
+        if (threadIdx.y == 0) {
+            int c = threadIdx.x;
+            for (int q = 0; q < (int)threadIdx.x && c == (int)threadIdx.x; ++q) {
+                bool same = true;
+                for (int i = 0; i < sup && same; ++i)
+                    same = __float_as_uint(sDx[q][i]) == __float_as_uint(sDx[threadIdx.x][i]);
+                if (same)
+                    c = q;
+            }
+            sColClass[threadIdx.x] = c;
+        }
+        if (threadIdx.x == 0) {
+            int c = threadIdx.y;
+            for (int q = 0; q < (int)threadIdx.y && c == (int)threadIdx.y; ++q) {
+                bool same = true;
+                for (int j = 0; j < sup && same; ++j)
+                    same = __float_as_uint(sDy[q][j]) == __float_as_uint(sDy[threadIdx.y][j]);
+                if (same)
+                    c = q;
+            }
+            sRowClass[threadIdx.y] = c;
+        }
+        __syncthreads();
+        if (t == 0) {
+            // compact group numbers in order of first appearance
+            int n = 0;
+            for (int q = 0; q < 32; ++q)
+                sColIdx[q] = sColClass[q] == q ? n++ : -1;
+            for (int q = 0; q < 32; ++q)
+                if (sColClass[q] != q)
+                    sColIdx[q] = sColIdx[sColClass[q]];
+            sColN = n;
+            n = 0;
+            for (int q = 0; q < 8; ++q)
+                sRowIdx[q] = sRowClass[q] == q ? n++ : -1;
+            for (int q = 0; q < 8; ++q)
+                if (sRowClass[q] != q)
+                    sRowIdx[q] = sRowIdx[sRowClass[q]];
+            sRowN = n;
+        }
+        __syncthreads();
+        const int nc = sColN, nr = sRowN, per = sup * sup;
+        tabled = nc * nr * per <= kRadialWeightsMax;
+        if (tabled) {
+            for (int k = t; k < nc * nr * per; k += nt) {
+                const int pair = k / per, tap = k - pair * per;
+                const int cg = pair % nc, rg = pair / nc;
+                // the representative column / row of each group
+                int qc = 0, qr = 0;
+                for (int q = 0; q < 32; ++q)
+                    if (sColClass[q] == q && sColIdx[q] == cg) { qc = q; break; }
+                for (int q = 0; q < 8; ++q)
+                    if (sRowClass[q] == q && sRowIdx[q] == rg) { qr = q; break; }
+                const float dx = sDx[qc][tap % sup], dy = sDy[qr][tap / sup];
+                sW[k] = (double)lutLookupShared(sLut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
+            }
+        }
     }
+    __syncthreads();
+    if (ox >= J.W || oy >= J.H)
+        return;
     double acc = 0.0, wsum = 0.0;
-    for (int j = 0; j < sup; ++j) {
-        const float dy = (float)((y0 + j - cy) * invW);
-        const int srow = (y0 + j - fy0) * fw - fx0;
-        const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
-        if (keepDx && tileStaged && lutStaged) {
-#pragma unroll
-            for (int i = 0; i < kRadialMaxSup; ++i) {
-                if (i >= sup)
-                    break;
-                const float dx = dxs[i];
-                const float w = lutLookupShared(sLut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
-                acc = fma((double)w, sY[srow + x0 + i], acc);
+    if (tabled) {
+        const double *w = sW + (size_t)(sRowIdx[threadIdx.y] * sColN + sColIdx[threadIdx.x]) * sup * sup;
+        for (int j = 0; j < sup; ++j) {
+            const double *srow = sY + (y0 + j - fy0) * fw + (x0 - fx0);
+            const double *wr = w + j * sup;
+            for (int i = 0; i < sup; ++i) {
+                acc = fma(wr[i], srow[i], acc);
+                wsum += wr[i];
+            }
+        }
+    } else {
+        for (int j = 0; j < sup; ++j) {
+            const float dy = (float)((y0 + j - cy) * invW);
+            const int srow = (y0 + j - fy0) * fw - fx0;
+            const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
+            for (int i = 0; i < sup; ++i) {
+                const float dx = (float)((x0 + i - cx) * invW);
+                const float r = sqrtf(dx * dx + dy * dy) * J.lutScale;
+                const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r)
+                                          : lutLookupDev(J.lut, J.lutN, r);
+                const double v = tileStaged ? sY[srow + x0 + i]
+                                            : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
+                acc = fma((double)w, v, acc);
                 wsum += (double)w;
             }
-            continue;
-        }
-        for (int i = 0; i < sup; ++i) {
-            const float dx = (float)((x0 + i - cx) * invW);
-            const float r = sqrtf(dx * dx + dy * dy) * J.lutScale;
-            const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r) : lutLookupDev(J.lut, J.lutN, r);
-            const double v = tileStaged ? sY[srow + x0 + i] : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
-            acc = fma((double)w, v, acc);
-            wsum += (double)w;
         }
     }
     storeLuma(J, ox, oy, (float)(wsum > 1e-6 ? acc / wsum : 0.0));
