@@ -352,6 +352,7 @@ __global__ void k_detail_plain(LGCR_STAGE_ARGS) {
     c.invWyC = J.sinvWyC;
     c.noClampX = J.sNoClampX;
     c.noClampY = J.sNoClampY;
+    c.uv = nullptr;
     float r, unused;
     plainAt(c, x, y, r, unused);
     J.detailTmp[o] = ldf(J.Y + o) - r;

@@ -1459,34 +1459,39 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
 
 // 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x8
 // block of output pixels stages the clamped input rows and columns its
-// windows cover (as doubles, the accumulation's operand type) and the
-// kernel's LUT in shared memory when they fit. A tap's weight depends only
-// on the pixel's column offsets (x0 + i - cx) / widen and row offsets
-// (y0 + j - cy) / widen as floats; the block groups its columns (and rows)
-// whose offset vectors are identical, evaluates the weights once per
-// (column group, row group) into a shared table of doubles, and every pixel
-// then accumulates from shared memory. The weights, their order and the FP64
-// accumulation are the reference's.
+// windows cover, as doubles (the accumulation's operand type). A tap's weight
+// depends only on the pixel's column offsets (x0 + i - cx) / widen and row
+// offsets (y0 + j - cy) / widen as floats, so warp 0 groups the block's
+// columns (and rows) whose offset vectors are identical, the block evaluates
+// the weights once per (column group, row group) into a shared table of
+// doubles, and every pixel accumulates from shared memory: one weight load,
+// one sample load and one FP64 FMA per tap. Blocks whose groups do not fit
+// the table evaluate each tap per pixel. The weights, their order and the
+// FP64 accumulation are the reference's.
 constexpr int kRadialTileMax = 2048;         // staged luma samples per block
-constexpr int kRadialLutMax = 4096;          // staged LUT entries
 constexpr int kRadialMaxSup = 16;            // offsets kept per column / row
 constexpr int kRadialWeightsMax = 1152;      // shared weight table (doubles)
 
-__device__ __forceinline__ float lutLookupShared(const float *lut, int n, float idx) {
-    int i0 = (int)idx;
-    i0 = iclamp(i0, 0, n - 2);
-    const float fr = smin(idx - (float)i0, 1.0f);
-    const float a = lut[i0];
-    return a + (lut[i0 + 1] - a) * fr;
+template <int SUP>
+__device__ __forceinline__ void radialTabled(const double *__restrict__ w, const double *__restrict__ s,
+                                             int fw, double &acc, double &wsum) {
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+#pragma unroll
+        for (int i = 0; i < SUP; ++i) {
+            const double wv = w[j * SUP + i];
+            acc = fma(wv, s[j * fw + i], acc);
+            wsum += wv;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256)
 k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     __shared__ double sY[kRadialTileMax];
-    __shared__ float sLut[kRadialLutMax];
     __shared__ double sW[kRadialWeightsMax];
     __shared__ float sDx[32][kRadialMaxSup], sDy[8][kRadialMaxSup];
-    __shared__ int sColClass[32], sRowClass[8], sColIdx[32], sRowIdx[8];
+    __shared__ int sColIdx[32], sRowIdx[8], sColRep[32], sRowRep[8];
     __shared__ int sColN, sRowN;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
@@ -1507,102 +1512,99 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     const int fw = (int)ceil((bxLast + 0.5) * sx - 0.5 - radius) + sup - fx0;
     const int fh = (int)ceil((byLast + 0.5) * sy - 0.5 - radius) + sup - fy0;
     const bool tileStaged = fw * fh <= kRadialTileMax;
-    const bool lutStaged = J.lutN <= kRadialLutMax;
-    const bool grouped = tileStaged && lutStaged && sup <= kRadialMaxSup;
+    const bool grouped = tileStaged && sup <= kRadialMaxSup;
     const int nt = blockDim.x * blockDim.y, t = threadIdx.y * blockDim.x + threadIdx.x;
     if (tileStaged)
         for (int k = t; k < fw * fh; k += nt)
             sY[k] = (double)ldf(J.Y + (size_t)iclamp(fy0 + k / fw, 0, J.sh - 1) * J.sw +
                                 iclamp(fx0 + k % fw, 0, J.sw - 1));
-    if (lutStaged)
-        for (int k = t; k < J.lutN; k += nt)
-            sLut[k] = ldf(J.lut + k);
     const double cy = (oy + 0.5) * sy - 0.5;
     const int y0 = (int)ceil(cy - radius);
     const double cx = (ox + 0.5) * sx - 0.5;
     const int x0 = (int)ceil(cx - radius);
-    bool tabled = false;
-    if (grouped) {
-        // offset vectors of the block's columns (row 0 of threads) and rows
-        // (column 0 of threads), then each one's first identical predecessor
-        if (threadIdx.y == 0)
-            for (int i = 0; i < sup; ++i)
-                sDx[threadIdx.x][i] = (float)((x0 + i - cx) * invW);
-        if (threadIdx.x == 0)
+    if (grouped && threadIdx.y == 0) {
+        // warp 0: lane l holds column l's offsets and, for l < 8, row l's;
+        // each column (row) joins the group of its first identical predecessor
+        const int lane = threadIdx.x;
+        for (int i = 0; i < sup; ++i)
+            sDx[lane][i] = (float)((x0 + i - cx) * invW);
+        if (lane < 8) {
+            const double ry = (by0 + lane + 0.5) * sy - 0.5;
+            const int ry0 = (int)ceil(ry - radius);
             for (int j = 0; j < sup; ++j)
-                sDy[threadIdx.y][j] = (float)((y0 + j - cy) * invW);
-        __syncthreads();
-        if (threadIdx.y == 0) {
-            int c = threadIdx.x;
-            for (int q = 0; q < (int)threadIdx.x && c == (int)threadIdx.x; ++q) {
-                bool same = true;
-                for (int i = 0; i < sup && same; ++i)
-                    same = __float_as_uint(sDx[q][i]) == __float_as_uint(sDx[threadIdx.x][i]);
-                if (same)
-                    c = q;
-            }
-            sColClass[threadIdx.x] = c;
+                sDy[lane][j] = (float)((ry0 + j - ry) * invW);
         }
-        if (threadIdx.x == 0) {
-            int c = threadIdx.y;
-            for (int q = 0; q < (int)threadIdx.y && c == (int)threadIdx.y; ++q) {
+        __syncwarp();
+        int c = lane;
+        for (int q = 0; q < lane && c == lane; ++q) {
+            bool same = true;
+            for (int i = 0; i < sup && same; ++i)
+                same = __float_as_uint(sDx[q][i]) == __float_as_uint(sDx[lane][i]);
+            if (same)
+                c = q;
+        }
+        int r = lane;
+        if (lane < 8)
+            for (int q = 0; q < lane && r == lane; ++q) {
                 bool same = true;
                 for (int j = 0; j < sup && same; ++j)
-                    same = __float_as_uint(sDy[q][j]) == __float_as_uint(sDy[threadIdx.y][j]);
+                    same = __float_as_uint(sDy[q][j]) == __float_as_uint(sDy[lane][j]);
                 if (same)
-                    c = q;
+                    r = q;
             }
-            sRowClass[threadIdx.y] = c;
+        const unsigned below = (1u << lane) - 1u;
+        const unsigned colReps = __ballot_sync(0xffffffffu, c == lane);
+        const unsigned rowReps = __ballot_sync(0xffffffffu, lane < 8 && r == lane);
+        // group number = rank of the representative among the representatives
+        const int myCol = __popc(colReps & below);
+        sColIdx[lane] = __shfl_sync(0xffffffffu, myCol, c);
+        if (c == lane)
+            sColRep[myCol] = lane;
+        const int myRow = __popc(rowReps & below);
+        const int rowIdx = __shfl_sync(0xffffffffu, myRow, lane < 8 ? r : 0);
+        if (lane < 8) {
+            sRowIdx[lane] = rowIdx;
+            if (r == lane)
+                sRowRep[myRow] = lane;
         }
-        __syncthreads();
-        if (t == 0) {
-            // compact group numbers in order of first appearance
-            int n = 0;
-            for (int q = 0; q < 32; ++q)
-                sColIdx[q] = sColClass[q] == q ? n++ : -1;
-            for (int q = 0; q < 32; ++q)
-                if (sColClass[q] != q)
-                    sColIdx[q] = sColIdx[sColClass[q]];
-            sColN = n;
-            n = 0;
-            for (int q = 0; q < 8; ++q)
-                sRowIdx[q] = sRowClass[q] == q ? n++ : -1;
-            for (int q = 0; q < 8; ++q)
-                if (sRowClass[q] != q)
-                    sRowIdx[q] = sRowIdx[sRowClass[q]];
-            sRowN = n;
-        }
-        __syncthreads();
-        const int nc = sColN, nr = sRowN, per = sup * sup;
-        tabled = nc * nr * per <= kRadialWeightsMax;
-        if (tabled) {
-            for (int k = t; k < nc * nr * per; k += nt) {
-                const int pair = k / per, tap = k - pair * per;
-                const int cg = pair % nc, rg = pair / nc;
-                // the representative column / row of each group
-                int qc = 0, qr = 0;
-                for (int q = 0; q < 32; ++q)
-                    if (sColClass[q] == q && sColIdx[q] == cg) { qc = q; break; }
-                for (int q = 0; q < 8; ++q)
-                    if (sRowClass[q] == q && sRowIdx[q] == rg) { qr = q; break; }
-                const float dx = sDx[qc][tap % sup], dy = sDy[qr][tap / sup];
-                sW[k] = (double)lutLookupShared(sLut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
-            }
+        if (lane == 0) {
+            sColN = __popc(colReps);
+            sRowN = __popc(rowReps);
         }
     }
     __syncthreads();
+    bool tabled = false;
+    if (grouped) {
+        const int nc = sColN, nr = sRowN, per = sup * sup;
+        tabled = nc * nr * per <= kRadialWeightsMax;
+        if (tabled)
+            for (int k = t; k < nc * nr * per; k += nt) {
+                const int pair = k / per, tap = k - pair * per;
+                const int qc = sColRep[pair % nc], qr = sRowRep[pair / nc];
+                const float dx = sDx[qc][tap % sup], dy = sDy[qr][tap / sup];
+                sW[k] = (double)lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
+            }
+        __syncthreads();
+    }
     if (ox >= J.W || oy >= J.H)
         return;
     double acc = 0.0, wsum = 0.0;
     if (tabled) {
         const double *w = sW + (size_t)(sRowIdx[threadIdx.y] * sColN + sColIdx[threadIdx.x]) * sup * sup;
-        for (int j = 0; j < sup; ++j) {
-            const double *srow = sY + (y0 + j - fy0) * fw + (x0 - fx0);
-            const double *wr = w + j * sup;
-            for (int i = 0; i < sup; ++i) {
-                acc = fma(wr[i], srow[i], acc);
-                wsum += wr[i];
-            }
+        const double *s = sY + (y0 - fy0) * fw + (x0 - fx0);
+        if (sup == 6) {
+            radialTabled<6>(w, s, fw, acc, wsum);
+        } else if (sup == 4) {
+            radialTabled<4>(w, s, fw, acc, wsum);
+        } else if (sup == 8) {
+            radialTabled<8>(w, s, fw, acc, wsum);
+        } else {
+            for (int j = 0; j < sup; ++j)
+                for (int i = 0; i < sup; ++i) {
+                    const double wv = w[j * sup + i];
+                    acc = fma(wv, s[j * fw + i], acc);
+                    wsum += wv;
+                }
         }
     } else {
         for (int j = 0; j < sup; ++j) {
@@ -1611,9 +1613,7 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
             const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
             for (int i = 0; i < sup; ++i) {
                 const float dx = (float)((x0 + i - cx) * invW);
-                const float r = sqrtf(dx * dx + dy * dy) * J.lutScale;
-                const float w = lutStaged ? lutLookupShared(sLut, J.lutN, r)
-                                          : lutLookupDev(J.lut, J.lutN, r);
+                const float w = lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
                 const double v = tileStaged ? sY[srow + x0 + i]
                                             : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
                 acc = fma((double)w, v, acc);

@@ -20,6 +20,7 @@ struct PlainCtx {
     int lutN;
     const float *lut;
     int noClampX, noClampY;      // every tap index of the axes is in range
+    const double2 *uv;           // p0 / p1 as FP64 pairs (chroma), or null
 };
 
 __device__ __forceinline__ void plainSeparableAt(const PlainCtx &c, int ox, int oy, float &o0, float &o1) {
@@ -105,6 +106,38 @@ __device__ __forceinline__ void plainRadialTable(const PlainCtx &c, int ox, int 
     const bool dual = c.p1 != nullptr;
     double acc0 = 0.0, acc1 = 0.0, wsum = 0.0, sumAbs = 0.0;
     float mn0 = 1e30f, mx0 = -1e30f, mn1 = 1e30f, mx1 = -1e30f;
+    if (dual && c.uv) {
+        // both planes from the FP64 pairs: one conversion per tap (the
+        // weight); the hull compares the exact double copies of the samples
+        double n0 = (double)mn0, x0d = (double)mx0, n1 = (double)mn1, x1d = (double)mx1;
+#pragma unroll
+        for (int j = 0; j < SUP; ++j) {
+            if (!((my >> j) & 1u))
+                continue;
+            const double2 *r = c.uv + (size_t)(ty0 + j) * c.w + tx0;
+            const float2 *wrow = reinterpret_cast<const float2 *>(base + j * SUP);
+#pragma unroll
+            for (int q = 0; q < SUP / 2; ++q) {
+                const float2 w2 = __ldg(wrow + q);
+                const float wk[2] = { w2.x, w2.y };
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = 2 * q + h;
+                    if (!((mx >> i) & 1u))
+                        continue;
+                    const double wd = (double)wk[h];
+                    const double2 p = __ldg(r + i);
+                    acc0 = fma(wd, p.x, acc0);
+                    wsum += wd;
+                    sumAbs += fabs(wd);
+                    n0 = smin(n0, p.x); x0d = smax(x0d, p.x);
+                    acc1 = fma(wd, p.y, acc1);
+                    n1 = smin(n1, p.y); x1d = smax(x1d, p.y);
+                }
+            }
+        }
+        mn0 = (float)n0; mx0 = (float)x0d; mn1 = (float)n1; mx1 = (float)x1d;
+    } else {
 #pragma unroll
     for (int j = 0; j < SUP; ++j) {
         if (!((my >> j) & 1u))
@@ -134,6 +167,7 @@ __device__ __forceinline__ void plainRadialTable(const PlainCtx &c, int ox, int 
                 }
             }
         }
+    }
     }
     double v0, v1 = 0.0;
     if (wsum > 1e-6 && wsum >= 0.05 * sumAbs) {
@@ -236,6 +270,7 @@ __device__ __forceinline__ PlainCtx chromaPlainCtx(const FrameJob &J) {
     c.margin = J.margin; c.invWxC = J.invWxC; c.invWyC = J.invWyC;
     c.lutScale = J.lutScale; c.lutN = J.lutN; c.lut = J.lut;
     c.noClampX = J.noClampX; c.noClampY = J.noClampY;
+    c.uv = reinterpret_cast<const double2 *>(J.uvd);
     return c;
 }
 
