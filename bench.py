@@ -508,7 +508,8 @@ def _gen_clip(task):
 def filters_leg(clip, dev, stream, steps, warmup):
     """Per-frame device-path throughput of Sharpen and TRecon (trad 1, every
     frame with its two neighbours) on a 1080p YUV420P10 clip resident in HBM,
-    beside the reference's AVX2 build on one host thread for one frame."""
+    and of Downsample (quality 0, 1, 2) on 1080p YUV444P10 frames, beside the
+    reference's AVX2 build on one host thread for one frame."""
     import numpy as np
     import torch
     from oracle import oracle as O
@@ -530,8 +531,7 @@ def filters_leg(clip, dev, stream, steps, warmup):
         for n in range(len(dclip)):
             trecon.frame(n, lambda i: dclip[i], out=outs, stream=h)
 
-    res = {}
-    for name, fn in (("sharpen", sharpen_pass), ("trecon", trecon_pass)):
+    def timed(fn, frames):
         for _ in range(max(warmup, 1)):
             fn()
         torch.cuda.synchronize(dev)
@@ -541,11 +541,28 @@ def filters_leg(clip, dev, stream, steps, warmup):
             fn()
         b.record(stream)
         torch.cuda.synchronize(dev)
-        ms = a.elapsed_time(b) / (steps * len(dclip))
+        ms = a.elapsed_time(b) / (steps * frames)
+        return {"ms_per_frame": round(ms, 3), "mpix_s": round(1920 * 1080 / (ms / 1000) / 1e6, 1)}
+
+    res = {}
+    for name, fn in (("sharpen", sharpen_pass), ("trecon", trecon_pass)):
         res[name] = {"workload": f"1920x1080 YUV420P10, {len(dclip)}-frame clip" +
                                  (", trad 1 (two neighbours)" if name == "trecon" else ""),
-                     "ms_per_frame": round(ms, 3),
-                     "mpix_s": round(1920 * 1080 / (ms / 1000) / 1e6, 1)}
+                     **timed(fn, len(dclip))}
+    # Downsample: 4:4:4 -> 4:2:0 of 1080p 10-bit frames (Mpix/s of source pixels)
+    f444 = S.FrameFormat(10, 0, 0)
+    ds_clip = [S.make_frame(1920, 1080, f444, seed=7000 + i) for i in range(4)]
+    ds_dev = [[torch.from_numpy(p.view(np.int16)).to(dev).view(torch.uint16) for p in f]
+              for f in ds_clip]
+    ds_out = [None] + [torch.empty((540, 960), dtype=torch.int16, device=dev).view(torch.uint16)
+                       for _ in range(2)]
+    for q in (0, 1, 2):
+        ds = lgcr.Downsample(lgcr.video_format(1920, 1080, 10, 0, 0), quality=q)
+        res[f"downsample_q{q}"] = {
+            "workload": f"1920x1080 YUV444P10 -> 4:2:0, quality {q}, spline36, strength 1, "
+                        f"{len(ds_dev)}-frame clip",
+            **timed(lambda: [ds.frame(f, out=ds_out, stream=h) for f in ds_dev], len(ds_dev))}
+        ds.close()
     if O.available("avx2"):
         t0 = time.perf_counter()
         O.sharpen(clip[1], 10, variant="avx2")
@@ -553,6 +570,11 @@ def filters_leg(clip, dev, stream, steps, warmup):
         t0 = time.perf_counter()
         O.trecon(clip[1], [clip[0], clip[2]], 10, len(clip), variant="avx2")
         res["trecon"]["cpu_reference_ms_per_frame"] = round(1000 * (time.perf_counter() - t0), 1)
+        for q in (0, 1, 2):
+            t0 = time.perf_counter()
+            O.downsample(ds_clip[0], bits=10, quality=q, variant="avx2")
+            res[f"downsample_q{q}"]["cpu_reference_ms_per_frame"] = round(
+                1000 * (time.perf_counter() - t0), 1)
         res["cpu_reference"] = "reference AVX2 build (oracle/_ref), one host thread, one frame"
     sharpen.close()
     trecon.close()
@@ -779,17 +801,19 @@ def roofline_of(stage_ms, kinds, algo_bytes, peaks, steps_note):
 
 def leg_only(args):
     """Profiler captures: run one leg alone (a configuration's batch, or the
-    Sharpen / TRecon clip) for `steps` graph replays after `warmup` and print
-    its time and stage split."""
+    Sharpen / TRecon / Downsample clips; "filters" prints all three) for
+    `steps` graph replays after `warmup` and print its time and stage
+    split."""
     global lgcr
     rank = 0
-    if args.leg in ("sharpen", "trecon"):
+    filter_legs = ("sharpen", "trecon", "downsample_q0", "downsample_q1", "downsample_q2", "filters")
+    if args.leg in filter_legs:
         with mp.get_context("spawn").Pool(1) as pool:
             clip = pool.map(_gen_clip, [(R.frame_seed(11000, rank, 0), FILTERS_CLIP)])[0]
     else:
         legs = leg_specs(rank)
         if args.leg not in legs:
-            raise SystemExit(f"unknown leg {args.leg!r}; one of {sorted(legs)} or sharpen, trecon")
+            raise SystemExit(f"unknown leg {args.leg!r}; one of {sorted(legs)} or {filter_legs}")
         leg = legs[args.leg]
         if leg.get("reuse_headline"):
             specs = [s for s in frame_specs(rank, args.frames) if s["width"] == 1920]
@@ -806,9 +830,9 @@ def leg_only(args):
     lib.lgcr_batch_stage_times.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.lgcr_stage_name.restype = ctypes.c_char_p
-    if args.leg in ("sharpen", "trecon"):
+    if args.leg in filter_legs:
         res = filters_leg(clip, dev, stream, args.steps, args.warmup)
-        print(json.dumps({"leg": args.leg, **res[args.leg]}))
+        print(json.dumps({"leg": args.leg, **(res if args.leg == "filters" else res[args.leg])}))
         return 0
     if args.leg_frames > 0:
         planes_list = planes_list[:args.leg_frames]

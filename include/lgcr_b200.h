@@ -274,6 +274,52 @@ int lgcr_trecon_frame(lgcr_trecon *filter, const lgcr_plane cur[3], const lgcr_p
                       void *stream);
 
 /* ---------------------------------------------------------------------
+ * Downsample: the reference's fourth filter, 4:4:4 -> 4:2:0 (8-16 bit or
+ * float). A separable polyphase base (spline36, lanczos3 or binomial) with
+ * a luma-guided correction near structure: quality 0 and 1 average the
+ * chroma along the luma's edge direction, quality 2 also scores four
+ * candidates by how well they re-upsample to the source chroma.
+ *   lgcr_downsample_create  <- downsampleCreate   src/downsample.cpp:820-911
+ *   lgcr_downsample_frame   <- downsampleGetFrame src/downsample.cpp:740-781
+ *   lgcr_downsample_destroy <- downsampleFree     src/downsample.cpp:814-818
+ * ------------------------------------------------------------------- */
+/* Downsample arguments, one field per entry of the reference signature
+ *   clip:vnode;quality:int:opt;kernel:data:opt;strength:float:opt;
+ *   loc:data:opt                       (src/downsample.cpp:913-918)
+ * quality LGCR_UNSET_INT, kernel / loc NULL and strength_set 0 mean "not
+ * given" (defaults 0, "spline36", 1.0, "left"); a given strength, NaN
+ * included, is validated like the reference's. */
+typedef struct lgcr_downsample_params {
+    int quality;
+    const char *kernel;       /* "spline36", "lanczos3" or "binomial"     */
+    double strength;
+    int strength_set;
+    const char *loc;          /* "left", "center", "topleft", "top",
+                                 "bottomleft" or "bottom"                  */
+} lgcr_downsample_params;
+
+typedef struct lgcr_downsample lgcr_downsample;
+
+void lgcr_downsample_params_init(lgcr_downsample_params *params);
+/* Validates like downsampleCreate (planar YUV 4:4:4, 8-16 bit integer or
+ * 32-bit float, even width and height: fmt->width/height must be given) and
+ * returns LGCR_E_INVALID with its message ("Downsample: input must be planar
+ * YUV444 (8-16 bit integer or float32)", ...). */
+int lgcr_downsample_create(const lgcr_downsample_params *params, const lgcr_format *fmt,
+                           lgcr_downsample **out, char *err, size_t errlen);
+void lgcr_downsample_destroy(lgcr_downsample *filter);
+/* The _ChromaLocation the output frames carry (0 left .. 5 bottom). */
+int lgcr_downsample_chroma_location(const lgcr_downsample *filter);
+/*
+ * One frame: in[0..2] the 4:4:4 Y, U, V planes; out[1], out[2] the
+ * (width/2) x (height/2) U and V planes. out[0].data NULL leaves luma to the
+ * caller (the reference shares the source's Y plane with the output frame);
+ * otherwise Y is copied to out[0]. memory and stream as for lgcr_recon_frame.
+ */
+int lgcr_downsample_frame(lgcr_downsample *filter, const lgcr_plane in[3], const lgcr_plane out[3],
+                          int memory, void *stream);
+
+/* ---------------------------------------------------------------------
  * Batched form: many frames (any mix of filters, sizes, subsamplings and
  * depths) in one launch per pipeline stage, captured as a CUDA graph and
  * replayed when the same batch layout is submitted again.

@@ -299,3 +299,43 @@ def trecon(cur, nbrs, bits=None, num_frames=None, chroma_location: int = -1,
           len(nbrs), _planes(outs), int(chroma_location), err, 512) != 0:
         raise OracleError(err.value.decode())
     return outs
+
+
+def downsample(planes, bits=None, variant: str = "scalar", quality=None, kernel=None,
+               strength=None, loc=None, color_family: int = 3, subsampling=(0, 0)):
+    """Reference Downsample of one frame: the reference's own downsampleCreate
+    and downsampleGetFrame (src/downsample.cpp:740-918), compiled unmodified
+    and driven by oracle/ds_host.cpp. `planes` are the 4:4:4 source planes;
+    returns (U, V, chroma_location) with U, V of (h/2, w/2) in the source's
+    sample type. Raises OracleError with the reference's message on invalid
+    arguments. `color_family` / `subsampling` override the source format, to
+    check the create-time validation."""
+    lib = library(variant)
+    fn = lib.oracle_downsample_frame
+    fn.argtypes = [ctypes.c_int] * 7 + [ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.c_longlong), ctypes.c_int,
+                                        ctypes.c_char_p, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int]
+    fn.restype = ctypes.c_int
+    planes = [np.ascontiguousarray(p) for p in planes]
+    dt = planes[0].dtype
+    is_float = dt == np.float32
+    if bits is None:
+        bits = 32 if is_float else (8 if dt == np.uint8 else 16)
+    h, w = planes[0].shape
+    ptrs = (ctypes.c_void_p * 3)(*[p.ctypes.data for p in planes])
+    strides = (ctypes.c_longlong * 3)(*[p.strides[0] for p in planes])
+    ou = np.zeros((h // 2, w // 2), dtype=dt)
+    ov = np.zeros((h // 2, w // 2), dtype=dt)
+    loc_out = ctypes.c_int(-1)
+    err = ctypes.create_string_buffer(512)
+    rc = fn(w, h, int(color_family), 1 if is_float else 0, int(bits), int(subsampling[0]),
+            int(subsampling[1]), ptrs, strides, UNSET_INT if quality is None else int(quality),
+            None if kernel is None else kernel.encode(),
+            0.0 if strength is None else float(strength), 0 if strength is None else 1,
+            None if loc is None else loc.encode(), ou.ctypes.data, ov.ctypes.data,
+            ctypes.byref(loc_out), err, 512)
+    if rc != 0:
+        raise OracleError(err.value.decode())
+    return ou, ov, loc_out.value

@@ -103,6 +103,8 @@ EXPORTS = (
     "lgcr_sharpen_params_init", "lgcr_sharpen_create", "lgcr_sharpen_frame",
     "lgcr_sharpen_destroy", "lgcr_trecon_params_init", "lgcr_trecon_create",
     "lgcr_trecon_neighbors", "lgcr_trecon_frame", "lgcr_trecon_destroy",
+    "lgcr_downsample_params_init", "lgcr_downsample_create", "lgcr_downsample_destroy",
+    "lgcr_downsample_chroma_location", "lgcr_downsample_frame",
 )
 
 _lib = None
@@ -458,6 +460,82 @@ class TRecon:
 def recon(planes, chroma_location: int = -1, bits=None, **kwargs):
     """One-shot Recon of a (Y, U, V) frame; returns the output planes."""
     return Recon(format_of(planes, bits), **kwargs).frame(planes, chroma_location)
+
+
+class DownsampleParams(ctypes.Structure):
+    _fields_ = [("quality", ctypes.c_int), ("kernel", ctypes.c_char_p),
+                ("strength", ctypes.c_double), ("strength_set", ctypes.c_int),
+                ("loc", ctypes.c_char_p)]
+
+
+class Downsample:
+    """The reference's `lgcr.Downsample` (downsampleCreate /
+    downsampleGetFrame, src/downsample.cpp:740-918): 4:4:4 -> 4:2:0 with a
+    luma-guided chroma correction. Arguments: quality (0..2), kernel
+    ("spline36", "lanczos3", "binomial"), strength (0..1), loc ("left",
+    "center", "topleft", "top", "bottomleft", "bottom"). `fmt` is the 4:4:4
+    source format with its (even) width and height."""
+
+    def __init__(self, fmt: Format, quality=None, kernel=None, strength=None, loc=None):
+        self.lib = library()
+        lib = self.lib
+        lib.lgcr_downsample_create.argtypes = [ctypes.POINTER(DownsampleParams),
+                                               ctypes.POINTER(Format),
+                                               ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                                               ctypes.c_size_t]
+        lib.lgcr_downsample_frame.argtypes = [ctypes.c_void_p, ctypes.POINTER(Plane),
+                                              ctypes.POINTER(Plane), ctypes.c_int, ctypes.c_void_p]
+        lib.lgcr_downsample_destroy.argtypes = [ctypes.c_void_p]
+        lib.lgcr_downsample_chroma_location.argtypes = [ctypes.c_void_p]
+        params = DownsampleParams(UNSET_INT if quality is None else int(quality),
+                                  None if kernel is None else kernel.encode(),
+                                  0.0 if strength is None else float(strength),
+                                  0 if strength is None else 1,
+                                  None if loc is None else loc.encode())
+        self.fmt = fmt
+        handle = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        if lib.lgcr_downsample_create(ctypes.byref(params), ctypes.byref(fmt),
+                                      ctypes.byref(handle), err, 512) != LGCR_OK:
+            raise Error(err.value.decode())
+        self.handle = handle
+        self.chroma_location = lib.lgcr_downsample_chroma_location(handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lgcr_downsample_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def frame(self, planes, out=None, stream=None):
+        """Downsample one frame: numpy planes through host memory, or CUDA
+        tensors enqueued on `stream` without waiting. Returns (Y, U, V); Y is
+        a copy of the source luma in `out[0]` (or the source plane itself
+        when out[0] is None)."""
+        device = hasattr(planes[0], "data_ptr")
+        if not device:
+            planes = [np.ascontiguousarray(p) for p in planes]
+        h, w = planes[0].shape
+        if out is None:
+            if device:
+                import torch
+                out = [None] + [torch.empty((h // 2, w // 2), dtype=planes[0].dtype,
+                                            device=planes[0].device) for _ in range(2)]
+            else:
+                out = [None] + [np.empty((h // 2, w // 2), dtype=planes[0].dtype)
+                                for _ in range(2)]
+        handle = getattr(stream, "cuda_stream", stream) if stream is not None else None
+        status = self.lib.lgcr_downsample_frame(self.handle, planes_desc(planes), planes_desc(out),
+                                                LGCR_MEM_DEVICE if device else LGCR_MEM_HOST,
+                                                handle)
+        if status != LGCR_OK:
+            raise Error(self.lib.lgcr_last_error().decode())
+        return [planes[0] if out[0] is None else out[0], out[1], out[2]]
 
 
 class Server:
