@@ -12,7 +12,9 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
   e2e          same metric through the per-frame C ABI (lgcr_recon_frame) with
                pinned host planes: H2D, run, D2H inside the timed region, one
                calling host thread per core (at most 16) like fmParallel
-               (e2e_pageable: the same with pageable host planes)
+               (e2e_pageable: the same with pageable host planes); its
+               copy_roofline is the step's H2D/D2H bytes over this box's
+               measured duplex pinned-copy rate
   per_frame    device-resident per-frame path (one lgcr_recon_frame per frame)
   roofline     dominant stage: algorithmic bytes of the frames its launch
                processes (9 B per output pixel for 10-bit 4:2:0 -> 4:4:4) / its
@@ -22,7 +24,8 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
                plain 720p, jinc resize and bm+bp configurations: batched and
                per-frame Mpix/s, stage split, roofline
   filters      Sharpen and TRecon (trad 1) per-frame device path on a 1080p
-               clip, beside the reference's AVX2 build on one thread
+               clip and Downsample (quality 0/1/2) on 1080p 4:4:4 frames,
+               beside the reference's AVX2 build on one thread
   cpu_baseline the reference's AVX2 build on this host's cores (bounded sample)
   serving      the serving configuration's mixed stream (5 frame kinds, algo
                2/4/6, bm on 10 %, 24 streams) as Poisson arrivals at 1.2x the
@@ -776,6 +779,45 @@ GUIDED_FP32_FLOP_PER_TAP = 27
 FP32_LANES_PER_SM, B200_SMS = 128, 148
 
 
+def link_bandwidth(dev, nbytes=256 << 20, reps=3):
+    """Host<->device copy rates of this box (pinned host memory, one large
+    copy per direction, CUDA events): H2D alone, D2H alone, and both at once
+    on two streams (the e2e leg's situation). GB/s; the e2e leg's copy
+    roofline is its per-step bytes over these rates."""
+    import torch
+    h_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    s1, s2 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+
+    def run(h2d, d2h):
+        start = torch.cuda.Event(enable_timing=True)
+        ends = []
+        start.record(s1)
+        s2.wait_event(start)
+        for on, stream, fn in ((h2d, s1, lambda: d_in.copy_(h_in, non_blocking=True)),
+                               (d2h, s2, lambda: h_out.copy_(d_out, non_blocking=True))):
+            if not on:
+                continue
+            with torch.cuda.stream(stream):
+                for _ in range(reps):
+                    fn()
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(stream)
+                ends.append(e)
+        torch.cuda.synchronize(dev)
+        return max(start.elapsed_time(e) for e in ends) / 1000.0
+
+    run(True, True)                                   # warm-up
+    gb = nbytes * reps / 1e9
+    h2d = gb / run(True, False)
+    d2h = gb / run(False, True)
+    both = run(True, True)
+    return {"h2d_gbs": round(h2d, 1), "d2h_gbs": round(d2h, 1),
+            "duplex_gbs_each": round(gb / both, 1)}
+
+
 def roofline_of(stage_ms, kinds, algo_bytes, peaks, steps_note):
     """Dominant stage: achieved algorithmic GB/s over the frames its launch
     processes vs the measured HBM copy bandwidth."""
@@ -1023,6 +1065,12 @@ def our_arm(args):
     e2e_page_s = R.max_over_ranks(time.perf_counter() - t0, dev)
     latencies[:] = e2e_latencies
     out_bytes_e2e = sum(2 * s["width"] * s["height"] * 2 for s in specs)   # U, V (luma shared)
+    # copy roofline of the e2e leg: its bytes per step over the measured
+    # duplex copy rate (both directions run at once)
+    link = link_bandwidth(dev)
+    copy_s = max(head.in_bytes, out_bytes_e2e) / (link["duplex_gbs_each"] * 1e9)
+    link["copy_bound_mpix_s"] = round(out_pixels * world / copy_s / 1e6, 1)
+    link["e2e_frac_of_copy_bound"] = round(e2e_value / link["copy_bound_mpix_s"], 3)
 
     # roofline of the dominant stage, with the guided stage's FP32 side
     kinds = [(s["algo"], True, False, False, False) for s in specs]
@@ -1070,7 +1118,8 @@ def our_arm(args):
                        "p99": round(sorted(latencies)[int(0.99 * (len(latencies) - 1))], 3)
                        if latencies else None, "per": "frame, e2e host path"},
         "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "host_threads": e2e_threads,
-                "h2d_bytes_per_step": int(head.in_bytes), "d2h_bytes_per_step": int(out_bytes_e2e)},
+                "h2d_bytes_per_step": int(head.in_bytes), "d2h_bytes_per_step": int(out_bytes_e2e),
+                "copy_roofline": link},
         "e2e_pageable": {"value": round(out_pixels * world * args.steps / e2e_page_s / 1e6, 2),
                          "unit": "Mpix/s", "host_threads": e2e_threads,
                          "buffers": "pageable numpy planes, staged by the library"},

@@ -9,6 +9,7 @@
 #include "impl.h"
 #include "kernels.cuh"
 
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -80,7 +81,7 @@ cudaEvent_t poolEvent(lgcr_batch *b) {
 }
 
 int ensureCapacity(lgcr_batch *b, int count) {
-    if (count <= b->capacity && size_t(stageCount()) * (count + 1) <= b->prefixCapacity)
+    if (count <= b->capacity && size_t(stageCount()) * (2 * count) <= b->prefixCapacity)
         return LGCR_OK;
     for (auto &sl : b->slots) {
         if (sl.pending)
@@ -89,7 +90,8 @@ int ensureCapacity(lgcr_batch *b, int count) {
         sl.release();
     }
     const int cap = std::max(count, 8);
-    b->prefixCapacity = size_t(stageCount()) * (cap + 1);
+    // room for one prefix table per frame group (at most one group per frame)
+    b->prefixCapacity = size_t(stageCount()) * (2 * cap);
     for (auto &sl : b->slots) {
         if (cudaMalloc(&sl.dJobs, sizeof(FrameJob) * cap) != cudaSuccess ||
             cudaHostAlloc((void **)&sl.hJobs, sizeof(FrameJob) * cap, cudaHostAllocDefault) != cudaSuccess ||
@@ -108,32 +110,97 @@ int ensureCapacity(lgcr_batch *b, int count) {
     return LGCR_OK;
 }
 
-// Launch sequence; with profiling, each launched stage is bracketed by events.
+// Frame groups of the stage sequence. Each group runs every stage before the
+// next group starts, so a group's intermediate planes can still be in L2
+// when its later stages read them; one group gives the fewest launches and
+// the shortest tails. Measured on one B200: frames that upscale (output at
+// least twice the source luma: 1080p -> 4K jinc) run their long guided pass
+// 14 % faster as groups of their own (their 1080p-sized inputs stay in L2),
+// while same-size frames are fastest as one group. By default every
+// upscaling frame is its own group and the frames between them form one;
+// LGCR_BATCH_GROUP=n (n >= 1) groups every n frames instead, 0 makes the
+// whole batch one group.
+int batchGroupFrames() {
+    static const int g = [] {
+        const char *e = std::getenv("LGCR_BATCH_GROUP");
+        return e ? std::max(0, std::atoi(e)) : -1;
+    }();
+    return g;
+}
+
+// The batch's frame groups and their stage plans; the plans' prefix tables
+// lie one after another in the slot's prefix buffer (offsets in ints).
+struct GroupedPlan {
+    std::vector<int> start;             // groups + 1 frame indices
+    std::vector<StagePlan> plans;
+    std::vector<size_t> offset;         // groups + 1
+};
+
+void planGroups(const std::vector<FrameJob> &jobs, GroupedPlan &gp) {
+    const int n = int(jobs.size());
+    const int g = batchGroupFrames();
+    gp.start.clear();
+    gp.plans.clear();
+    gp.offset.assign(1, 0);
+    if (g >= 0) {
+        for (int f = 0; f < n; f += (g > 0 ? g : n))
+            gp.start.push_back(f);
+    } else {
+        auto upscale = [&](int f) {
+            return (long long)jobs[f].W * jobs[f].H >= 2LL * jobs[f].sw * jobs[f].sh;
+        };
+        for (int f = 0; f < n; ++f)
+            if (f == 0 || upscale(f) || upscale(f - 1))
+                gp.start.push_back(f);
+    }
+    gp.start.push_back(n);
+    const int groups = int(gp.start.size()) - 1;
+    gp.plans.resize(groups);
+    for (int k = 0; k < groups; ++k) {
+        const std::vector<FrameJob> sub(jobs.begin() + gp.start[k], jobs.begin() + gp.start[k + 1]);
+        planStages(sub, gp.plans[k]);
+        gp.offset.push_back(gp.offset.back() + gp.plans[k].prefix.size());
+    }
+}
+
+// Launch sequence, group by group; with profiling, each launched stage is
+// bracketed by events.
 int enqueue(lgcr_batch *b, DescriptorSlot &sl, const std::vector<FrameJob> &jobs,
-            const StagePlan &plan, cudaStream_t s) {
+            const GroupedPlan &gp, cudaStream_t s) {
     const int n = int(jobs.size());
     if (cudaMemcpyAsync(sl.dJobs, sl.hJobs, sizeof(FrameJob) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(sl.dPrefix, sl.hPrefix, plan.prefix.size() * sizeof(int),
+        cudaMemcpyAsync(sl.dPrefix, sl.hPrefix, gp.offset.back() * sizeof(int),
                         cudaMemcpyHostToDevice, s) != cudaSuccess)
         return -1;
-    if (!b->profiling)
-        return launchStages(jobs, plan, sl.dJobs, sl.dPrefix, s);
-    // profiled: one stage at a time so each launch gets its own events
     int launches = 0;
-    StagePlan single = plan;
-    for (int st = 0; st < stageCount(); ++st) {
-        if (plan.totals[st] == 0)
+    for (size_t k = 0; k + 1 < gp.start.size(); ++k) {
+        const std::vector<FrameJob> sub(jobs.begin() + gp.start[k], jobs.begin() + gp.start[k + 1]);
+        const StagePlan &plan = gp.plans[k];
+        const FrameJob *dJobs = sl.dJobs + gp.start[k];
+        const int *dPrefix = sl.dPrefix + gp.offset[k];
+        if (!b->profiling) {
+            const int l = launchStages(sub, plan, dJobs, dPrefix, s);
+            if (l < 0)
+                return -1;
+            launches += l;
             continue;
-        for (int o = 0; o < stageCount(); ++o)
-            single.totals[o] = (o == st) ? plan.totals[st] : 0;
-        StageEvent ev{st, poolEvent(b), poolEvent(b)};
-        cudaEventRecord(ev.start, s);
-        const int l = launchStages(jobs, single, sl.dJobs, sl.dPrefix, s);
-        cudaEventRecord(ev.stop, s);
-        if (l < 0)
-            return -1;
-        launches += l;
-        b->events.push_back(ev);
+        }
+        // profiled: one stage at a time so each launch gets its own events
+        StagePlan single = plan;
+        for (int st = 0; st < stageCount(); ++st) {
+            if (plan.totals[st] == 0)
+                continue;
+            for (int o = 0; o < stageCount(); ++o)
+                single.totals[o] = (o == st) ? plan.totals[st] : 0;
+            StageEvent ev{st, poolEvent(b), poolEvent(b)};
+            cudaEventRecord(ev.start, s);
+            const int l = launchStages(sub, single, dJobs, dPrefix, s);
+            cudaEventRecord(ev.stop, s);
+            if (l < 0)
+                return -1;
+            launches += l;
+            b->events.push_back(ev);
+        }
     }
     return launches;
 }
@@ -232,10 +299,13 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
                       t.out[0].data != nullptr, jobs[i].inKind);
         sig += buf;
     }
-    StagePlan plan;
-    planStages(jobs, plan);
+    GroupedPlan plan;
+    planGroups(jobs, plan);
     std::memcpy(sl.hJobs, jobs.data(), sizeof(FrameJob) * count);
-    std::memcpy(sl.hPrefix, plan.prefix.data(), plan.prefix.size() * sizeof(int));
+    for (size_t k = 0; k < plan.plans.size(); ++k)
+        std::memcpy(sl.hPrefix + plan.offset[k], plan.plans[k].prefix.data(),
+                    plan.plans[k].prefix.size() * sizeof(int));
+    sig += "|g" + std::to_string(plan.plans.size());
     int launches = -1;
     // the legacy default stream cannot be captured: its runs launch directly
     const bool capturable = s != nullptr && s != cudaStreamLegacy;

@@ -40,14 +40,20 @@ struct Request {
     int batchSize = 0;
 };
 
+// Staging planes of one batch position of a lane. They grow to the largest
+// frame the position has seen, in stream order on the lane's stream: a
+// stream-ordered free and allocation do not synchronize the device, so a
+// mixed stream growing its slots never stalls the other lanes' batches.
 struct DeviceSlot {
+    cudaStream_t stream = nullptr;
     void *in[3] = {nullptr, nullptr, nullptr};
     void *out[3] = {nullptr, nullptr, nullptr};
     size_t inBytes[3] = {0, 0, 0}, outBytes[3] = {0, 0, 0};
+    explicit DeviceSlot(cudaStream_t s) : stream(s) {}
     ~DeviceSlot() {
         for (int i = 0; i < 3; ++i) {
-            if (in[i]) cudaFree(in[i]);
-            if (out[i]) cudaFree(out[i]);
+            if (in[i]) cudaFreeAsync(in[i], stream);
+            if (out[i]) cudaFreeAsync(out[i], stream);
         }
     }
     bool ensure(int p, bool isIn, size_t bytes) {
@@ -55,10 +61,10 @@ struct DeviceSlot {
         size_t &have = isIn ? inBytes[p] : outBytes[p];
         if (have >= bytes)
             return true;
-        if (ptr) cudaFree(ptr);
+        if (ptr) cudaFreeAsync(ptr, stream);
         ptr = nullptr;
         have = 0;
-        if (cudaMalloc(&ptr, bytes) != cudaSuccess)
+        if (cudaMallocAsync(&ptr, bytes, stream) != cudaSuccess)
             return false;
         have = bytes;
         return true;
@@ -149,7 +155,7 @@ void laneLoop(lgcr_server *S, int laneIndex) {
         std::vector<lgcr_batch_item> items(take.size());
         for (size_t i = 0; i < take.size() && status == LGCR_OK; ++i) {
             Request *r = take[i];
-            if (!slots[i]) slots[i] = std::make_unique<DeviceSlot>();
+            if (!slots[i]) slots[i] = std::make_unique<DeviceSlot>(stream);
             const int bps = r->filter->filter->bytesPerSample();
             items[i].filter = r->filter;
             items[i].chroma_location = r->chromaLocation;
@@ -202,6 +208,7 @@ void laneLoop(lgcr_server *S, int laneIndex) {
     }
     lgcr_batch_destroy(batch);
     slots.clear();
+    cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
 }
 
