@@ -150,6 +150,21 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 # reference arm: the reference's AVX2 CPU build on the host cores
 # ---------------------------------------------------------------------------
+def host_cpu():
+    """CPU model and logical core count of this host (for the CPU baselines)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_logical_cores": os.cpu_count() or 1,
+            "usable_cores": cpu_threads()}
+
+
 def cpu_threads():
     try:
         n = len(os.sched_getaffinity(0))
@@ -327,7 +342,7 @@ def reference_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": {"workload": WORKLOAD, "frames_per_step": per_step},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": sample, **host_cpu()},
         "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -774,9 +789,33 @@ def axis_active_means(f):
 
 
 # FP32 arithmetic of one guided tap (tapsSeparable in kernels_recon.cu): 27
-# FP32 FLOPs (an FMA counted as 2) and 2 reciprocal approximations.
+# FP32 FLOPs (an FMA counted as 2) and 2 reciprocal approximations; with a
+# jinc phase table the base weight is read instead of formed as wx * wy (26).
 GUIDED_FP32_FLOP_PER_TAP = 27
+GUIDED_FP32_FLOP_PER_RADIAL_TAP = 26
 FP32_LANES_PER_SM, B200_SMS = 128, 148
+
+
+def guided_fp32(rl, filt, active, kinds, sm_mhz):
+    """When the dominant stage is the guided pass, add its counted FP32 work
+    against the nominal FP32 rate: taps = active guided pixels x mean active
+    taps per column x per row (the reference's tap metric, recon.cpp:253-257)."""
+    if not rl or rl["kernel"] != "reconstructChroma":
+        return
+    mx, my = axis_active_means(filt)
+    guided = stage_frames("reconstructChroma", kinds)
+    taps = sum(active[i] for i in guided) * mx * my
+    per_tap = GUIDED_FP32_FLOP_PER_RADIAL_TAP if filt.radial else GUIDED_FP32_FLOP_PER_TAP
+    fp32_peak = B200_SMS * FP32_LANES_PER_SM * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+    achieved_tf = taps * per_tap / (rl["launch_ms"] / 1000.0) / 1e12
+    rl["binding_bound"] = ("instruction issue and load latency of the FP32 (packed pairs), "
+                           "FP64 accumulation and reciprocal pipes")
+    rl["fp32"] = {"achieved_tflops": round(achieved_tf, 2), "peak_tflops": round(fp32_peak, 1),
+                  "frac": round(achieved_tf / fp32_peak, 4),
+                  "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 FLOP x sampled SM clock",
+                  "taps_per_step": int(taps),
+                  "taps_source": "active guided pixels x mean active taps per column x per row",
+                  "flop_per_tap": per_tap}
 
 
 def link_bandwidth(dev, nbytes=256 << 20, reps=3):
@@ -1077,21 +1116,7 @@ def our_arm(args):
     sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
     rl = roofline_of(stage_ms, kinds, head.algo_bytes, peaks,
                      f"event-bracketed pass of {prof_steps} steps")
-    if rl and rl["kernel"] == "reconstructChroma":
-        mx, my = axis_active_means(head_filters[0])
-        guided = stage_frames("reconstructChroma", kinds)
-        taps = sum(active[i] for i in guided) * mx * my
-        flops = taps * GUIDED_FP32_FLOP_PER_TAP
-        fp32_peak = B200_SMS * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
-        achieved_tf = flops / (rl["launch_ms"] / 1000.0) / 1e12
-        rl["binding_bound"] = ("instruction issue of the FP32 (packed pairs), FP64 "
-                               "accumulation and reciprocal pipes")
-        rl["fp32"] = {"achieved_tflops": round(achieved_tf, 2), "peak_tflops": round(fp32_peak, 1),
-                      "frac": round(achieved_tf / fp32_peak, 4),
-                      "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 FLOP x sampled SM clock",
-                      "taps_per_step": int(taps),
-                      "taps_source": "active guided pixels x mean active taps per column x per row",
-                      "flop_per_tap": GUIDED_FP32_FLOP_PER_TAP}
+    guided_fp32(rl, head_filters[0], active, kinds, sm_mhz)
 
     result = {
         "metric": METRIC, "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
@@ -1148,10 +1173,12 @@ def our_arm(args):
             b.per_frame()
             pms = b.timed(b.per_frame, leg_steps)
             sms = b.stage_split(2)
-            lr, _ = b.sparse_active()
+            lr, la = b.sparse_active()
             fa = leg["filter"]
             kinds = [(fa.get("algo", 2), fa.get("strength", 0.8) > 0, bool(fa.get("bm")),
                       fa.get("bp", 0.0) > 0, "width" in fa)] * len(lf)
+            leg_rl = roofline_of(sms, kinds, b.algo_bytes, peaks, "event-bracketed pass of 2 steps")
+            guided_fp32(leg_rl, lf[0], la, kinds, (clocks or {}).get("sm_mhz"))
             out_legs[name] = {
                 "workload": leg["workload"], "frames": len(lf),
                 "batched": {"value": round(b.out_pixels * leg_steps / (bms / 1000) / 1e6, 2),
@@ -1161,8 +1188,7 @@ def our_arm(args):
                 "batched_vs_per_frame": round(pms / max(bms, 1e-9), 3),
                 "sparse_active_ratio": round(float(np.mean(lr)), 4),
                 "launches_per_step": lib.lgcr_batch_launch_count(b.batch),
-                "roofline": roofline_of(sms, kinds, b.algo_bytes, peaks,
-                                        "event-bracketed pass of 2 steps")}
+                "roofline": leg_rl}
             b.close()
             del lf
         result["legs"] = out_legs
@@ -1186,6 +1212,7 @@ def our_arm(args):
             "sample": f"{len(times)} rounds of {threads} frames (alternating 1080p/4K, algo 2/6, "
                       f"one frame per thread) from the workload, reference AVX2 build "
                       f"(oracle/_ref), {total_s:.1f} s",
+            **host_cpu(),
             "reference_scene": reference_scene_fps()}
     if world > 1:
         torch.distributed.barrier()

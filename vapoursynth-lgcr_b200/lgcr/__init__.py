@@ -242,6 +242,8 @@ class Recon:
         out = Format()
         self.lib.lgcr_recon_output_format(self.handle, ctypes.byref(out))
         self.out_w, self.out_h = out.width, out.height
+        # the jinc kernel is the radial (2D) path
+        self.radial = kwargs.get("kernel") == "jinc"
 
     def close(self):
         if getattr(self, "handle", None):
