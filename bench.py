@@ -717,6 +717,18 @@ class BatchLeg:
         self.algo_bytes = [algorithmic_bytes(p, f.out_w, f.out_h) for f, p in zip(filters, planes_list)]
         self.in_bytes = sum(sum(p.nbytes for p in planes) for planes in planes_list)
 
+    def tune(self):
+        """This batch's own autotuner (block shapes, guided variant, frame
+        grouping) on its frames; untimed. Returns the report lines."""
+        import torch
+        rep = ctypes.create_string_buffer(8192)
+        st = self.lib.lgcr_batch_autotune(self.batch, self.items, len(self.filters),
+                                          ctypes.c_void_p(self.stream.cuda_stream), rep, 8192)
+        torch.cuda.synchronize(self.dev)
+        if st != 0:
+            raise RuntimeError(self.lib.lgcr_last_error().decode())
+        return [l for l in rep.value.decode().splitlines() if l]
+
     def run(self, use_graph=1):
         st = self.lib.lgcr_batch_run(self.batch, self.items, len(self.filters),
                                      ctypes.c_void_p(self.stream.cuda_stream), use_graph)
@@ -920,13 +932,14 @@ def leg_only(args):
     filters = [lgcr.Recon(lgcr.format_of(p, 10 if leg.get("reuse_headline") else None),
                           **leg["filter"]) for p in planes_list]
     b = BatchLeg(lib, dev, stream, filters, planes_list)
+    tuned = [] if args.no_autotune else b.tune()
     for _ in range(max(args.warmup, 1)):
         b.run(1)
     torch.cuda.synchronize(dev)
     ms = b.timed(lambda: b.run(1), args.steps)
     stage_ms = b.stage_split(1)
     b.close()
-    print(json.dumps({"leg": args.leg, "frames": len(filters),
+    print(json.dumps({"leg": args.leg, "frames": len(filters), "autotune": tuned,
                       "ms_per_step": round(ms / args.steps, 3),
                       "mpix_s": round(b.out_pixels * args.steps / (ms / 1000) / 1e6, 1),
                       "stage_ms_per_step": {k: round(v, 3) for k, v in
@@ -990,6 +1003,8 @@ def our_arm(args):
         if lib.lgcr_autotune(head.items, len(specs), ctypes.c_void_p(stream.cuda_stream), rep, 4096) == 0:
             tuned = rep.value.decode()
         torch.cuda.synchronize(dev)
+        # then the headline batch's own settings (frame grouping included)
+        tuned += "\n".join("batch " + l for l in head.tune())
 
     # warm-up (tables, workspaces, the graphs of this layout)
     for _ in range(max(args.warmup, 1)):
@@ -1166,6 +1181,7 @@ def our_arm(args):
             lf = [lgcr.Recon(lgcr.format_of(p, 10 if leg.get("reuse_headline") else None),
                              **leg["filter"]) for p in planes_list]
             b = BatchLeg(lib, dev, stream, lf, planes_list)
+            leg_tuned = [] if args.no_autotune else b.tune()
             for _ in range(max(args.warmup, 1)):
                 b.run(1)
             barrier()
@@ -1188,6 +1204,7 @@ def our_arm(args):
                 "batched_vs_per_frame": round(pms / max(bms, 1e-9), 3),
                 "sparse_active_ratio": round(float(np.mean(lr)), 4),
                 "launches_per_step": lib.lgcr_batch_launch_count(b.batch),
+                "autotune": leg_tuned,
                 "roofline": leg_rl}
             b.close()
             del lf

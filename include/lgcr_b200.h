@@ -2,7 +2,8 @@
  * lgcr_b200.h — C ABI of the B200-native LGCR Recon implementation.
  *
  * This is the drop-in boundary for the `lgcr.Recon` path of
- * MysteryDove/vapoursynth-LGCR.  Every entry point takes plain pointers,
+ * MysteryDove/vapoursynth-LGCR and its Sharpen, TRecon and Downsample
+ * filters.  Every entry point takes plain pointers,
  * sizes and strides; no CUDA, VapourSynth or torch types appear in the
  * signatures (a CUDA stream is passed as `void *`).
  *
@@ -17,6 +18,8 @@
  *                             src/plugin.cpp:14-111
  *   lgcr_trecon_*          <- tReconCreate / tReconGetFrame
  *                             src/plugin.cpp:723-990
+ *   lgcr_downsample_*      <- downsampleCreate / downsampleGetFrame /
+ *                             downsampleFree src/downsample.cpp:740-918
  *   lgcr_server_*          <- the VapourSynth core's concurrent request
  *                             scheduling of Recon frames (no single
  *                             reference symbol; see plugin.cpp:215-217
@@ -172,7 +175,9 @@ const char *lgcr_last_error(void);
  * Work is enqueued on `stream` (a cudaStream_t) and the call does not wait
  * for the GPU to run it; its uploads of the geometry tables and the frame
  * descriptor read pageable host memory, so the call may block the host until
- * those few kilobytes are staged.
+ * those few kilobytes are staged. A call on a stream that is being captured
+ * into a CUDA graph returns LGCR_E_ARGUMENT (the copies would read host
+ * memory the call has released).
  */
 int lgcr_recon_frame_static(lgcr_recon *filter, const lgcr_plane in[3],
                             const lgcr_plane out[3], int chroma_location, void *stream);
@@ -353,8 +358,20 @@ int lgcr_batch_stage_times(lgcr_batch *batch, double *ms, int *launches, int res
 int lgcr_stage_count(void);
 const char *lgcr_stage_name(int stage);
 
+/* Per-batch autotuner: on the given items (the layout about to be run),
+ * times the candidate block shapes of the tunable per-pixel stages, the
+ * guided kernel's variants and the frame grouping of the stage sequence,
+ * and keeps the fastest for this batch only (later runs of `batch` use
+ * them; other batches and the per-frame path are unaffected). Runs the
+ * items several times on `stream` and waits for them; report (optional)
+ * receives one line per tuned choice. */
+int lgcr_batch_autotune(lgcr_batch *batch, const lgcr_batch_item *items, int count,
+                        void *stream, char *report, size_t reportlen);
+
 /* Autotuner: time the candidate launch shapes of every stage on the
- * given items and keep the fastest per stage (process-wide). */
+ * given items and keep the fastest per stage (process-wide: frames planned
+ * afterwards use them; plans already made keep the settings they were
+ * planned with). */
 int lgcr_autotune(const lgcr_batch_item *items, int count, void *stream,
                   char *report, size_t reportlen);
 

@@ -130,3 +130,29 @@ def test_static_rejects_oversize_and_unsupported():
     o8 = [torch.zeros((48, 64), dtype=torch.uint8, device="cuda") for _ in range(3)]
     assert fn(bm.handle, lgcr.planes_desc(p8), lgcr.planes_desc(o8), -1, stream) != 0
     assert "bm" in lib.lgcr_last_error().decode()
+
+
+def test_static_call_refuses_stream_capture():
+    """Its table uploads read host memory the call releases, so a call on a
+    capturing stream is refused (nothing enqueued) instead of leaving copy
+    nodes that a replay would run on freed memory."""
+    import warnings
+    lib, fn = bind()
+    w, h = 128, 64
+    rec = lgcr.Recon(lgcr.video_format(w, h, 10, 1, 1), algo=2, kernel="lanczos", taps=4)
+    dev = to_device(S.make_frame(w, h, S.YUV420P10, seed=91))
+    outs = empty_like_out(rec, dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    assert fn(rec.handle, lgcr.planes_desc(dev), lgcr.planes_desc(outs), -1, stream) == 0
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")          # the captured graph stays empty
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            status = fn(rec.handle, lgcr.planes_desc(dev), lgcr.planes_desc(outs), -1,
+                        torch.cuda.current_stream().cuda_stream)
+    assert status != 0
+    assert "captured" in lib.lgcr_last_error().decode()
+    # the filter still works outside the capture
+    assert fn(rec.handle, lgcr.planes_desc(dev), lgcr.planes_desc(outs), -1, stream) == 0
+    torch.cuda.synchronize()

@@ -57,6 +57,12 @@ struct lgcr_batch {
     std::vector<cudaEvent_t> eventPool;
     std::vector<double> stageMs;
     std::vector<int> stageLaunches;
+    // this batch's own launch settings (lgcr_batch_autotune); until tuned,
+    // every run plans with the process-wide settings
+    bool ownConfig = false;
+    LaunchConfig cfg{};
+    int groupMode = -2;                 // -2: process default (see batchGroupFrames)
+    int cfgVersion = 0;                 // part of the graph signature
     ~lgcr_batch() {
         for (auto &sl : slots) {
             sl.release();
@@ -136,9 +142,11 @@ struct GroupedPlan {
     std::vector<size_t> offset;         // groups + 1
 };
 
-void planGroups(const std::vector<FrameJob> &jobs, GroupedPlan &gp) {
+// groupMode: -1 upscaling frames alone, 0 one group, n >= 1 every n frames
+void planGroups(const std::vector<FrameJob> &jobs, GroupedPlan &gp, int groupMode,
+                const LaunchConfig *cfg) {
     const int n = int(jobs.size());
-    const int g = batchGroupFrames();
+    const int g = groupMode;
     gp.start.clear();
     gp.plans.clear();
     gp.offset.assign(1, 0);
@@ -158,7 +166,7 @@ void planGroups(const std::vector<FrameJob> &jobs, GroupedPlan &gp) {
     gp.plans.resize(groups);
     for (int k = 0; k < groups; ++k) {
         const std::vector<FrameJob> sub(jobs.begin() + gp.start[k], jobs.begin() + gp.start[k + 1]);
-        planStages(sub, gp.plans[k]);
+        planStages(sub, gp.plans[k], cfg);
         gp.offset.push_back(gp.offset.back() + gp.plans[k].prefix.size());
     }
 }
@@ -300,12 +308,14 @@ int lgcr_batch_run(lgcr_batch *b, const lgcr_batch_item *items, int count, void 
         sig += buf;
     }
     GroupedPlan plan;
-    planGroups(jobs, plan);
+    planGroups(jobs, plan, b->groupMode >= -1 ? b->groupMode : batchGroupFrames(),
+               b->ownConfig ? &b->cfg : nullptr);
     std::memcpy(sl.hJobs, jobs.data(), sizeof(FrameJob) * count);
     for (size_t k = 0; k < plan.plans.size(); ++k)
         std::memcpy(sl.hPrefix + plan.offset[k], plan.plans[k].prefix.data(),
                     plan.plans[k].prefix.size() * sizeof(int));
-    sig += "|g" + std::to_string(plan.plans.size());
+    sig += "|g" + std::to_string(plan.plans.size()) + "|c" +
+           std::to_string(b->ownConfig ? b->cfgVersion : -1 - processConfigVersion());
     int launches = -1;
     // the legacy default stream cannot be captured: its runs launch directly
     const bool capturable = s != nullptr && s != cudaStreamLegacy;
@@ -474,6 +484,135 @@ extern "C" int lgcr_autotune(const lgcr_batch_item *items, int count, void *stre
             text += line + " -> " + names[bestV] + "\n";
     }
     lgcr_batch_destroy(b);
+    if (report && reportlen) {
+        std::strncpy(report, text.c_str(), reportlen - 1);
+        report[reportlen - 1] = '\0';
+    }
+    return status;
+}
+
+// Per-batch autotuner: tunes this batch's own launch settings on the given
+// items (the layout the caller will run) without touching the process-wide
+// settings, so other batches and per-frame calls keep running unchanged:
+//  * the block shape of every tunable per-pixel stage the items use
+//    (stage-event time of that stage);
+//  * the persistent guided kernel's variant (its stage-event time);
+//  * the frame grouping of the stage sequence (whole-run time, events around
+//    three runs): upscaling frames alone, one group, or one frame per group.
+// Later runs of this batch plan with the chosen settings and re-capture their
+// graphs.
+extern "C" int lgcr_batch_autotune(lgcr_batch *b, const lgcr_batch_item *items, int count,
+                                   void *stream, char *report, size_t reportlen) {
+    static const int cand[][2] = {{32, 8}, {16, 8}, {32, 4}, {64, 4}, {16, 16}, {128, 2}, {8, 8}};
+    static const char *variantNames[3] = {"2-blocks", "3-blocks", "staged"};
+    if (!b || !items || count <= 0) {
+        setError("LGCR: empty batch");
+        return LGCR_E_ARGUMENT;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool wasProfiling = b->profiling;
+    if (!b->ownConfig) {
+        b->cfg = processLaunchConfig();
+        b->ownConfig = true;
+    }
+    if (b->groupMode < -1)
+        b->groupMode = batchGroupFrames();
+    std::vector<double> ms(stageCount());
+    int status = LGCR_OK;
+    // one untimed run, then two timed ones: stage times per run
+    auto stageRun = [&]() {
+        status = lgcr_batch_run(b, items, count, stream, 0);
+        lgcr_batch_stage_times(b, nullptr, nullptr, 1);
+        for (int rep = 0; rep < 2 && status == LGCR_OK; ++rep)
+            status = lgcr_batch_run(b, items, count, stream, 0);
+        lgcr_batch_stage_times(b, ms.data(), nullptr, 1);
+        for (double &v : ms)
+            v /= 2.0;
+    };
+    std::string text;
+    b->profiling = true;
+    for (int st = 0; st < stageCount() && status == LGCR_OK; ++st) {
+        if (!stageTunable(st))
+            continue;
+        int bestX = b->cfg.shapeX[st], bestY = b->cfg.shapeY[st];
+        double best = 1e300;
+        std::string line = std::string(stageName(st)) + ":";
+        for (const auto &c : cand) {
+            b->cfg.shapeX[st] = c[0];
+            b->cfg.shapeY[st] = c[1];
+            stageRun();
+            if (status != LGCR_OK || ms[st] <= 0.0)
+                break;                          // stage not used by these items
+            char buf[64];
+            std::snprintf(buf, sizeof(buf), " %dx%d=%.3fms", c[0], c[1], ms[st]);
+            line += buf;
+            if (ms[st] < best) { best = ms[st]; bestX = c[0]; bestY = c[1]; }
+        }
+        b->cfg.shapeX[st] = bestX;
+        b->cfg.shapeY[st] = bestY;
+        if (best < 1e300) {
+            char buf[48];
+            std::snprintf(buf, sizeof(buf), " -> %dx%d\n", bestX, bestY);
+            text += line + buf;
+        }
+    }
+    int guidedStage = -1;
+    for (int st = 0; st < stageCount(); ++st)
+        if (std::string(stageName(st)) == "reconstructChroma")
+            guidedStage = st;
+    if (status == LGCR_OK && guidedStage >= 0) {
+        int bestV = b->cfg.guidedVariant;
+        double best = 1e300;
+        std::string line = "reconstructChroma:";
+        for (int v = 0; v < 3 && status == LGCR_OK; ++v) {
+            b->cfg.guidedVariant = v;
+            stageRun();
+            if (status != LGCR_OK || ms[guidedStage] <= 0.0)
+                break;
+            char buf[64];
+            std::snprintf(buf, sizeof(buf), " %s=%.3fms", variantNames[v], ms[guidedStage]);
+            line += buf;
+            if (ms[guidedStage] < best) { best = ms[guidedStage]; bestV = v; }
+        }
+        b->cfg.guidedVariant = bestV;
+        if (best < 1e300)
+            text += line + " -> " + variantNames[bestV] + "\n";
+    }
+    // frame grouping: whole runs between events, profiling off
+    b->profiling = false;
+    if (status == LGCR_OK) {
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        static const int modes[3] = {-1, 0, 1};
+        static const char *modeNames[3] = {"upscaling-alone", "one-group", "per-frame"};
+        int bestMode = b->groupMode;
+        double best = 1e300;
+        std::string line = "frame groups:";
+        for (int m = 0; m < 3 && status == LGCR_OK; ++m) {
+            b->groupMode = modes[m];
+            status = lgcr_batch_run(b, items, count, stream, 0);
+            cudaEventRecord(t0, s);
+            for (int rep = 0; rep < 3 && status == LGCR_OK; ++rep)
+                status = lgcr_batch_run(b, items, count, stream, 0);
+            cudaEventRecord(t1, s);
+            float t = 0.0f;
+            if (status != LGCR_OK || cudaEventSynchronize(t1) != cudaSuccess ||
+                cudaEventElapsedTime(&t, t0, t1) != cudaSuccess)
+                break;
+            char buf[64];
+            std::snprintf(buf, sizeof(buf), " %s=%.3fms", modeNames[m], t / 3.0);
+            line += buf;
+            if (t < best) { best = t; bestMode = modes[m]; }
+        }
+        b->groupMode = bestMode;
+        if (best < 1e300)
+            text += line + " -> " + modeNames[bestMode == -1 ? 0 : bestMode == 0 ? 1 : 2] + "\n";
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+    }
+    b->profiling = wasProfiling;
+    ++b->cfgVersion;                    // graphs of earlier settings are re-captured
     if (report && reportlen) {
         std::strncpy(report, text.c_str(), reportlen - 1);
         report[reportlen - 1] = '\0';

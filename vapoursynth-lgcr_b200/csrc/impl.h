@@ -169,14 +169,31 @@ void buildJob(const FrameTask &t, FrameJob &job);
 // device copy of `jobs`; `dPrefix` receives the stage prefix tables (space
 // for stageCount * (n + 1) ints) and is written from `hPrefix` (pinned,
 // same size) by one copy. Returns the number of kernel launches, or -1.
+// Launch settings a plan is made and launched with: block shapes of the
+// tunable per-pixel stages and the persistent guided kernel's variant. A
+// plan keeps its own copy, so its tile counts and block shapes always agree
+// even when the settings change while it runs.
+constexpr int kMaxStages = 64;
+struct LaunchConfig {
+    int shapeX[kMaxStages], shapeY[kMaxStages];
+    int guidedVariant;
+};
+// The process-wide settings (lgcr_autotune, LGCR_GUIDED_VARIANT) and a
+// counter that changes whenever they do.
+LaunchConfig processLaunchConfig();
+int processConfigVersion();
+
 struct StagePlan {
     std::vector<int> prefix;            // stageCount * (n+1)
     std::vector<int> totals;            // blocks per stage
     int maxDil = 0;
     int nyqPasses = 0;
+    LaunchConfig cfg;
 };
 int stageCount();
-void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan);
+// cfg == nullptr: the process-wide settings at the time of the call
+void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan,
+                const LaunchConfig *cfg = nullptr);
 int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan,
                  const FrameJob *dJobs, const int *dPrefix, cudaStream_t stream);
 

@@ -1158,6 +1158,20 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
         else
             tapsSeparable<4, false>(c, tx0, ty0, wxp, wyp, maskBits(amx, 4), maskBits(amy, 4),
                                     l0, u0, c.cw, a);
+    } else if (fastRadial && win) {
+        // the warp staged rows ty0 .. ty0 + sup - 1 around every pixel's columns
+        const float *l0 = win->lc + (tx0 - win->tx0);
+        const double2 *u0 = win->uv + (tx0 - win->tx0);
+        const float *rad = radialWeightsAt(J.rad, ox, oy);
+        if (ax.sup == 6)
+            tapsSeparable<6, true, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 6),
+                                         maskBits(amy, 6), l0, u0, kStageCols, a, rad);
+        else if (ax.sup == 8)
+            tapsSeparable<8, true, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 8),
+                                         maskBits(amy, 8), l0, u0, kStageCols, a, rad);
+        else
+            tapsSeparable<4, true, true>(c, tx0, ty0, nullptr, nullptr, maskBits(amx, 4),
+                                         maskBits(amy, 4), l0, u0, kStageCols, a, rad);
     } else if (fastRadial) {
         const float *l0 = c.lc + (size_t)ty0 * c.cw + tx0;
         const double2 *u0 = c.uv + (size_t)ty0 * c.cw + tx0;
@@ -1340,7 +1354,10 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
                 const int loMin = __reduce_min_sync(0xffffffffu, lo);
                 const int loMax = __reduce_max_sync(0xffffffffu, lo);
                 const int sup = J.ax.sup;
-                bool ok = all && loMin == loMax && !J.radial && J.noClampX && J.noClampY &&
+                // separable frames, and jinc frames with a phase table (the
+                // radial tap loop reads the same staged window)
+                const bool radialOk = !J.radial || (J.rad.valid && J.rad.supX == sup && J.rad.supY == sup);
+                bool ok = all && loMin == loMax && radialOk && J.noClampX && J.noClampY &&
                           sup == J.ay.sup && sup <= kStageRows && sup >= 4 && !(sup & 1);
                 int tx0 = 0, ty0 = 0, txMin = 0, txMax = 0, tyMin = 0, tyMax = 0;
                 if (ok) {                                   // warp-uniform
@@ -1384,7 +1401,8 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
 
 // Register budgets of the same persistent kernel: 2 resident blocks per SM
 // (no spills) or 3 (fewer registers, a few spills), and 2 blocks with the
-// warps' tap windows staged in shared memory; the autotuner picks.
+// warps' tap windows (separable or jinc) staged in shared memory; the
+// autotuner picks.
 __global__ void __launch_bounds__(256, 2)
 k_guided(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;

@@ -845,10 +845,15 @@ void stageShape(int s, int &bx, int &by) {
     bx = gShapeX[s]; by = gShapeY[s];
 }
 
+static std::atomic<int> gConfigVersion{0};
+
+int processConfigVersion() { return gConfigVersion.load(); }
+
 void setStageShape(int s, int bx, int by) {
     std::lock_guard<std::mutex> lock(gShapeMu);
     initShapes();
     gShapeX[s] = bx; gShapeY[s] = by;
+    gConfigVersion.fetch_add(1);
 }
 
 // Variant of the persistent guided kernel (0: 2 blocks/SM, 1: 3 blocks/SM,
@@ -868,16 +873,30 @@ int guidedVariant() {
 void setGuidedVariant(int v) {
     std::lock_guard<std::mutex> lock(gShapeMu);
     gGuidedVariant = (v >= 0 && v <= 2) ? v : 0;
+    gConfigVersion.fetch_add(1);
+}
+
+static_assert(S_N <= kMaxStages, "LaunchConfig holds every stage");
+
+LaunchConfig processLaunchConfig() {
+    LaunchConfig c;
+    for (int s = 0; s < kMaxStages; ++s) {
+        c.shapeX[s] = 32;
+        c.shapeY[s] = 8;
+    }
+    for (int s = 0; s < S_N; ++s)
+        stageShape(s, c.shapeX[s], c.shapeY[s]);
+    c.guidedVariant = guidedVariant();
+    return c;
 }
 
 static int stageTilesShaped(const FrameJob &J, int s);
 
-static int stageTiles(const FrameJob &J, int s) {
+static int stageTiles(const FrameJob &J, int s, const LaunchConfig &cfg) {
     if (stageTunable(s)) {
         const int base = stageTilesShaped(J, s);
         if (base == 0) return 0;
-        int bx, by;
-        stageShape(s, bx, by);
+        const int bx = cfg.shapeX[s], by = cfg.shapeY[s];
         switch (s) {
         case S_DET_TRANSFER: case S_BM_AGG: return cdiv(J.W, bx) * cdiv(J.H, by);
         case S_HPASS: return cdiv(J.W, bx) * cdiv(J.ch, by);
@@ -932,8 +951,9 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     return 0;
 }
 
-void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan) {
+void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan, const LaunchConfig *cfg) {
     const int n = int(jobs.size());
+    plan.cfg = cfg ? *cfg : processLaunchConfig();
     plan.prefix.assign(size_t(S_N) * (n + 1), 0);
     plan.totals.assign(S_N, 0);
     plan.maxDil = 0;
@@ -941,7 +961,7 @@ void planStages(const std::vector<FrameJob> &jobs, StagePlan &plan) {
         int acc = 0;
         for (int f = 0; f < n; ++f) {
             plan.prefix[size_t(s) * (n + 1) + f] = acc;
-            acc += stageTiles(jobs[f], s);
+            acc += stageTiles(jobs[f], s, plan.cfg);
         }
         plan.prefix[size_t(s) * (n + 1) + n] = acc;
         plan.totals[s] = acc;
@@ -960,11 +980,8 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     auto go = [&](int s, auto kernel, dim3 block, size_t smem = 0) {
         if (plan.totals[s] == 0)
             return;
-        if (stageTunable(s)) {
-            int bx, by;
-            stageShape(s, bx, by);
-            block = dim3(bx, by);
-        }
+        if (stageTunable(s))
+            block = dim3(plan.cfg.shapeX[s], plan.cfg.shapeY[s]);
         kernel<<<plan.totals[s], block, smem, stream>>>(dJobs, pre(s), n);
         ++launches;
     };
@@ -995,7 +1012,7 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_PLAIN, k_plain, b32x8, kPlainDynSmem);
     if (plan.totals[S_GUIDED] > 0) {
         // persistent grid: enough resident blocks to fill every SM
-        const int variant = guidedVariant();
+        const int variant = plan.cfg.guidedVariant;
         static int gridBlocks[3] = {0, 0, 0};
         const size_t dyn = variant == 2 ? kGuidedStageBytes : 0;
         if (gridBlocks[variant] == 0) {

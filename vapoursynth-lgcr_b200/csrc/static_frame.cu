@@ -78,6 +78,15 @@ extern "C" int lgcr_recon_frame_static(lgcr_recon *h, const lgcr_plane in[3],
         setError("LGCR: null argument");
         return LGCR_E_ARGUMENT;
     }
+    // the uploads read host memory that is gone when the call returns: a
+    // captured copy node would read it again at every replay
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing((cudaStream_t)stream, &capturing) == cudaSuccess &&
+        capturing != cudaStreamCaptureStatusNone) {
+        setError("LGCR: lgcr_recon_frame_static cannot be captured into a CUDA graph "
+                 "(its table uploads read host memory owned by the call)");
+        return LGCR_E_ARGUMENT;
+    }
     Filter &F = *h->filter;
     const FilterParams q = F.sited(chroma_location);
     if (q.bm || F.needsBackProjection(q) || (q.strength > 0.0 && q.algo != 2)) {

@@ -98,7 +98,7 @@ EXPORTS = (
     "lgcr_params_init", "lgcr_recon_create", "lgcr_recon_destroy",
     "lgcr_recon_output_format", "lgcr_recon_frame", "lgcr_last_error",
     "lgcr_batch_create", "lgcr_batch_destroy", "lgcr_batch_run",
-    "lgcr_batch_launch_count", "lgcr_autotune",
+    "lgcr_batch_launch_count", "lgcr_autotune", "lgcr_batch_autotune",
     "lgcr_server_create", "lgcr_server_submit", "lgcr_server_wait", "lgcr_server_destroy",
     "lgcr_sharpen_params_init", "lgcr_sharpen_create", "lgcr_sharpen_frame",
     "lgcr_sharpen_destroy", "lgcr_trecon_params_init", "lgcr_trecon_create",
@@ -144,6 +144,8 @@ def library():
         "lgcr_stage_name": ([ctypes.c_int], ctypes.c_char_p),
         "lgcr_autotune": ([ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_void_p,
                            ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "lgcr_batch_autotune": ([ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_int,
+                                 ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
         "lgcr_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)],
                                ctypes.c_int),
         "lgcr_server_submit": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Plane),
