@@ -878,15 +878,25 @@ void setGuidedVariant(int v) {
 
 static_assert(S_N <= kMaxStages, "LaunchConfig holds every stage");
 
+// One lock for the whole snapshot: every frame plan takes one, from as many
+// host threads as call the library at once.
 LaunchConfig processLaunchConfig() {
     LaunchConfig c;
     for (int s = 0; s < kMaxStages; ++s) {
         c.shapeX[s] = 32;
         c.shapeY[s] = 8;
     }
-    for (int s = 0; s < S_N; ++s)
-        stageShape(s, c.shapeX[s], c.shapeY[s]);
-    c.guidedVariant = guidedVariant();
+    std::lock_guard<std::mutex> lock(gShapeMu);
+    initShapes();
+    for (int s = 0; s < S_N; ++s) {
+        c.shapeX[s] = gShapeX[s];
+        c.shapeY[s] = gShapeY[s];
+    }
+    if (gGuidedVariant < 0) {
+        const char *e = std::getenv("LGCR_GUIDED_VARIANT");
+        gGuidedVariant = (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 0;
+    }
+    c.guidedVariant = gGuidedVariant;
     return c;
 }
 
