@@ -903,10 +903,63 @@ __device__ __forceinline__ void windowHullInRange(const FrameJob &J, int tx0, in
     h[0] = maxAbsDL; h[1] = mnU; h[2] = mxU; h[3] = mnV; h[4] = mxV;
 }
 
+// Pass 1 fused with the radial plain base of the same window (jinc frames
+// whose selector needs the plain sample): the active taps are the plain
+// pass's too (same axis activity and window start), so one traversal gives
+// the guided hull and luma range and the plain sums of plainRadialTable
+// (phase-table weights, FP64 in the same tap order). The hull comes from
+// the FP64 copies of the samples (the same values as the float planes).
+struct RadialPlainSums {
+    double u, v, wsum, sumAbs;
+};
+
+template <int SUP>
+__device__ __forceinline__ void windowHullPlainRadial(const FrameJob &J, int tx0, int ty0,
+                                                      const uint8_t *amx, const uint8_t *amy, float L0,
+                                                      const float *base, float *h, RadialPlainSums &ps) {
+    const uint32_t mx = maskBits(amx, SUP), my = maskBits(amy, SUP);
+    const double2 *uvd = reinterpret_cast<const double2 *>(J.uvd);
+    float maxAbsDL = 0.0f;
+    double mnU = 1e30, mxU = -1e30, mnV = 1e30, mxV = -1e30;
+    double au = 0.0, av = 0.0, ws = 0.0, wa = 0.0;
+#pragma unroll
+    for (int j = 0; j < SUP; ++j) {
+        if (!((my >> j) & 1u))
+            continue;
+        const size_t row = (size_t)(ty0 + j) * J.cw + tx0;
+        const float2 *wrow = reinterpret_cast<const float2 *>(base + j * SUP);
+#pragma unroll
+        for (int q = 0; q < SUP / 2; ++q) {
+            const float2 w2 = __ldg(wrow + q);
+            const float wk[2] = { w2.x, w2.y };
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = 2 * q + k;
+                if (!((mx >> i) & 1u))
+                    continue;
+                const float l = ldf(J.lc + row + i);
+                const double2 p = __ldg(uvd + row + i);
+                maxAbsDL = smax(maxAbsDL, fabsf(l - L0));
+                mnU = smin(mnU, p.x); mxU = smax(mxU, p.x);
+                mnV = smin(mnV, p.y); mxV = smax(mxV, p.y);
+                const double wd = (double)wk[k];
+                au = fma(wd, p.x, au);
+                av = fma(wd, p.y, av);
+                ws += wd;
+                wa += fabs(wd);
+            }
+        }
+    }
+    h[0] = maxAbsDL; h[1] = (float)mnU; h[2] = (float)mxU; h[3] = (float)mnV; h[4] = (float)mxV;
+    ps.u = au; ps.v = av; ps.wsum = ws; ps.sumAbs = wa;
+}
+
 struct Guided {
     double u, v;
     float L0, ssRamp, guideFade, nx, ny;
     bool hasDir;
+    bool havePlain;                     // plainU/V hold the plain base
+    float plainU, plainV;
 };
 
 // A warp's guided-tap window staged in shared memory: kStageRows x
@@ -989,7 +1042,40 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     const uint8_t *amy = ay.am + (size_t)oy * ay.sup;
     float maxAbsDL = 0.0f;
     float hMinU = 1e30f, hMaxU = -1e30f, hMinV = 1e30f, hMaxV = -1e30f;
-    if (J.wHull) {
+    g.havePlain = false;
+    g.plainU = g.plainV = 0.0f;
+    // jinc frames whose integer-output selector needs the plain base
+    const bool fusePlain = J.radial && J.algo == 4 && J.outKind != kF32 && J.rad.valid &&
+                           J.rad.supX == ax.sup && J.rad.supY == ay.sup && J.noClampX &&
+                           J.noClampY && ax.sup == ay.sup &&
+                           (ax.sup == 4 || ax.sup == 6 || ax.sup == 8);
+    if (fusePlain) {
+        float h[5];
+        RadialPlainSums ps;
+        const float *rbase = radialWeightsAt(J.rad, ox, oy);
+        switch (ax.sup) {
+        case 4: windowHullPlainRadial<4>(J, tx0, ty0, amx, amy, L0, rbase, h, ps); break;
+        case 6: windowHullPlainRadial<6>(J, tx0, ty0, amx, amy, L0, rbase, h, ps); break;
+        default: windowHullPlainRadial<8>(J, tx0, ty0, amx, amy, L0, rbase, h, ps); break;
+        }
+        maxAbsDL = h[0]; hMinU = h[1]; hMaxU = h[2]; hMinV = h[3]; hMaxV = h[4];
+        // the plain base's finish (plainRadialTable in plain.cuh)
+        double v0, v1;
+        if (ps.wsum > 1e-6 && ps.wsum >= 0.05 * ps.sumAbs) {
+            v0 = ps.u / ps.wsum;
+            v1 = ps.v / ps.wsum;
+        } else {
+            v0 = bilinearAt(J.U, cw, ch, __ldg(ax.pos + ox), __ldg(ay.pos + oy));
+            v1 = bilinearAt(J.V, cw, ch, __ldg(ax.pos + ox), __ldg(ay.pos + oy));
+        }
+        if (J.clampHull) {
+            v0 = sclamp(v0, (double)(hMinU - J.margin), (double)(hMaxU + J.margin));
+            v1 = sclamp(v1, (double)(hMinV - J.margin), (double)(hMaxV + J.margin));
+        }
+        g.havePlain = true;
+        g.plainU = (float)v0;
+        g.plainV = (float)v1;
+    } else if (J.wHull) {
         hMinU = wHull.x; hMaxU = wHull.y; hMinV = wHull.z; hMaxV = wHull.w;
         maxAbsDL = smax(maxAbsDL, fabsf(wLum.y - L0));
         maxAbsDL = smax(maxAbsDL, fabsf(wLum.x - L0));
@@ -1237,7 +1323,12 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
     if (J.outKind != kF32) {
         // integer output: single-expression fused selector on the plain base
         float baseU, baseV;
-        plainPixel(J, ox, oy, baseU, baseV);
+        if (g.havePlain) {
+            baseU = g.plainU;
+            baseV = g.plainV;
+        } else {
+            plainPixel(J, ox, oy, baseU, baseV);
+        }
         double valueU, valueV;
         if (w2 >= 1e-4f || w3 >= 1e-4f) {
             const int cx = __ldg(J.ax.cbI0 + ox), cy = __ldg(J.ay.cbI0 + oy);
