@@ -432,6 +432,14 @@ __device__ __forceinline__ void extremaFromRows(const FrameJob &J, const float4 
     J.wLum[o] = make_float2(mnL, mxL);
 }
 
+// Jinc selector frames whose guided pass also forms the radial plain base of
+// its listed pixels (guidedPixel's pass 1): the plain stage skips those.
+__device__ __forceinline__ bool radialPlainFused(const FrameJob &J) {
+    return J.guided && J.radial && J.algo == 4 && J.rad.valid && J.rad.supX == J.ax.sup &&
+           J.rad.supY == J.ay.sup && J.noClampX && J.noClampY && J.ax.sup == J.ay.sup &&
+           (J.ax.sup == 4 || J.ax.sup == 6 || J.ax.sup == 8);
+}
+
 // Plain stage: every pixel the guided pass does not finalize. A block covers
 // 32 output columns x J.plainRows output rows. For the separable kernels it
 // needs the horizontal entries of the chroma rows its windows touch:
@@ -473,7 +481,7 @@ k_plain(LGCR_STAGE_ARGS) {
     const bool fused = J.plainFused && (separable || J.listed);
     const bool table = separable && (J.hTab || fused);
     const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
-    const bool skipListed = J.listed && !floatSelector;
+    const bool skipListed = J.listed && (!floatSelector || radialPlainFused(J));
     int syLo = 0, nRows = 0;
     if (table || fused) {
         const int oyLast = oy0 + rowsHere - 1;
@@ -1044,11 +1052,9 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     float hMinU = 1e30f, hMaxU = -1e30f, hMinV = 1e30f, hMaxV = -1e30f;
     g.havePlain = false;
     g.plainU = g.plainV = 0.0f;
-    // jinc frames whose integer-output selector needs the plain base
-    const bool fusePlain = J.radial && J.algo == 4 && J.outKind != kF32 && J.rad.valid &&
-                           J.rad.supX == ax.sup && J.rad.supY == ay.sup && J.noClampX &&
-                           J.noClampY && ax.sup == ay.sup &&
-                           (ax.sup == 4 || ax.sup == 6 || ax.sup == 8);
+    // jinc selector frames: the plain base of the listed pixels comes from
+    // this pass (the plain stage skips them)
+    const bool fusePlain = radialPlainFused(J);
     if (fusePlain) {
         float h[5];
         RadialPlainSums ps;
@@ -1350,7 +1356,17 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
         return;
     }
     // float output: routing metadata; blended after the ROI-limited LGF
-    const float baseU = J.oU[o], baseV = J.oV[o];
+    float baseU, baseV;
+    if (g.havePlain) {
+        // the plain base of this listed pixel, for the blend stage too
+        baseU = g.plainU;
+        baseV = g.plainV;
+        J.oU[o] = baseU;
+        J.oV[o] = baseV;
+    } else {
+        baseU = J.oU[o];
+        baseV = J.oV[o];
+    }
     const bool compressed = J.sparse &&
         (unsigned long long)J.counters[kCntActiveOutput] * 2ull < (unsigned long long)J.W * J.H;
     if (compressed) {
