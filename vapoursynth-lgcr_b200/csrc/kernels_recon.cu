@@ -432,14 +432,6 @@ __device__ __forceinline__ void extremaFromRows(const FrameJob &J, const float4 
     J.wLum[o] = make_float2(mnL, mxL);
 }
 
-// Jinc selector frames whose guided pass also forms the radial plain base of
-// its listed pixels (guidedPixel's pass 1): the plain stage skips those.
-__device__ __forceinline__ bool radialPlainFused(const FrameJob &J) {
-    return J.guided && J.radial && J.algo == 4 && J.rad.valid && J.rad.supX == J.ax.sup &&
-           J.rad.supY == J.ay.sup && J.noClampX && J.noClampY && J.ax.sup == J.ay.sup &&
-           (J.ax.sup == 4 || J.ax.sup == 6 || J.ax.sup == 8);
-}
-
 // Plain stage: every pixel the guided pass does not finalize. A block covers
 // 32 output columns x J.plainRows output rows. For the separable kernels it
 // needs the horizontal entries of the chroma rows its windows touch:
@@ -980,6 +972,10 @@ struct StagedWindow {
     int tx0, ty0;
 };
 
+// RFUSE: the kernel instance for batches with jinc selector frames (their
+// pass 1 also forms the plain base); the other instance has no such code, so
+// the separable frames' tap loops keep their schedule.
+template <bool RFUSE>
 __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
                                               const StagedWindow *win) {
     const AxisView &ax = J.ax, &ay = J.ay;
@@ -1054,7 +1050,7 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     g.plainU = g.plainV = 0.0f;
     // jinc selector frames: the plain base of the listed pixels comes from
     // this pass (the plain stage skips them)
-    const bool fusePlain = radialPlainFused(J);
+    const bool fusePlain = RFUSE && radialPlainFused(J);
     if (fusePlain) {
         float h[5];
         RadialPlainSums ps;
@@ -1313,9 +1309,10 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
 }
 
 // One listed pixel: algo 2 output, or the algo 4 selector (recon.cpp:762-811).
+template <bool RFUSE>
 __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
                                            const StagedWindow *win) {
-    const Guided g = guidedPixel(J, ox, oy, win);
+    const Guided g = guidedPixel<RFUSE>(J, ox, oy, win);
     if (J.algo == 2) {
         emit(J, ox, oy, (float)g.u, (float)g.v);
         return;
@@ -1329,7 +1326,7 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
     if (J.outKind != kF32) {
         // integer output: single-expression fused selector on the plain base
         float baseU, baseV;
-        if (g.havePlain) {
+        if (RFUSE && g.havePlain) {
             baseU = g.plainU;
             baseV = g.plainV;
         } else {
@@ -1357,7 +1354,7 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
     }
     // float output: routing metadata; blended after the ROI-limited LGF
     float baseU, baseV;
-    if (g.havePlain) {
+    if (RFUSE && g.havePlain) {
         // the plain base of this listed pixel, for the blend stage too
         baseU = g.plainU;
         baseV = g.plainV;
@@ -1416,7 +1413,7 @@ __device__ __forceinline__ void cpAsyncWaitAll() {
 static_assert(kGuidedStageBytes == size_t(8) * kStageRows * kStageCols * (4 + 16),
               "staged guided windows: 8 warps x kStageRows x kStageCols x (lc + (u, v))");
 
-template <int MIN_BLOCKS, bool STAGED>
+template <int MIN_BLOCKS, bool STAGED, bool RFUSE>
 __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, int njobs) {
     __shared__ unsigned long long pre[kGuidedMaxFrames + 1];
     extern __shared__ __align__(16) unsigned char guidedStage[];
@@ -1498,7 +1495,7 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
                 }
             }
             if (valid)
-                guidedWork(J, ox, oy, win);
+                guidedWork<RFUSE>(J, ox, oy, win);
             if (STAGED)
                 __syncwarp();                       // the slice is rewritten next round
         }
@@ -1513,19 +1510,38 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
 __global__ void __launch_bounds__(256, 2)
 k_guided(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
-    guidedGrid<2, false>(jobs, njobs);
+    guidedGrid<2, false, false>(jobs, njobs);
 }
 
 __global__ void __launch_bounds__(256, 3)
 k_guided3(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
-    guidedGrid<3, false>(jobs, njobs);
+    guidedGrid<3, false, false>(jobs, njobs);
 }
 
 __global__ void __launch_bounds__(256, 2)
 k_guided_staged(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
-    guidedGrid<2, true>(jobs, njobs);
+    guidedGrid<2, true, false>(jobs, njobs);
+}
+
+// the same three for batches with jinc selector frames
+__global__ void __launch_bounds__(256, 2)
+k_guided_r(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2, false, true>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 3)
+k_guided3_r(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<3, false, true>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 2)
+k_guided_staged_r(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2, true, true>(jobs, njobs);
 }
 
 // Float output planes -> typed output (output conversion stage).
@@ -1582,9 +1598,10 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
     storeLuma(J, x, y, (float)acc);
 }
 
-// 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x8
-// block of output pixels stages the clamped input rows and columns its
-// windows cover, as doubles (the accumulation's operand type). A tap's weight
+// 2D jinc luma resize (resampleRadial, src/kernels.cpp:276-334). A 32x32
+// tile of output pixels (256 threads, four rows each) stages the clamped
+// input rows and columns its windows cover, as doubles (the accumulation's
+// operand type). A tap's weight
 // depends only on the pixel's column offsets (x0 + i - cx) / widen and row
 // offsets (y0 + j - cy) / widen as floats, so warp 0 groups the block's
 // columns (and rows) whose offset vectors are identical, the block evaluates
@@ -1593,6 +1610,7 @@ __global__ void k_luma_v(const FrameJob *__restrict__ jobs, const int *__restric
 // one sample load and one FP64 FMA per tap. Blocks whose groups do not fit
 // the table evaluate each tap per pixel. The weights, their order and the
 // FP64 accumulation are the reference's.
+constexpr int kRadialBx = 32, kRadialBy = 32; // output tile of one block
 constexpr int kRadialTileMax = 2048;         // staged luma samples per block
 constexpr int kRadialMaxSup = 16;            // offsets kept per column / row
 constexpr int kRadialWeightsMax = 1152;      // shared weight table (doubles)
@@ -1615,15 +1633,15 @@ __global__ void __launch_bounds__(256)
 k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     __shared__ double sY[kRadialTileMax];
     __shared__ double sW[kRadialWeightsMax];
-    __shared__ float sDx[32][kRadialMaxSup], sDy[8][kRadialMaxSup];
-    __shared__ int sColIdx[32], sRowIdx[8], sColRep[32], sRowRep[8];
+    __shared__ float sDx[kRadialBx][kRadialMaxSup], sDy[kRadialBy][kRadialMaxSup];
+    __shared__ int sColIdx[kRadialBx], sRowIdx[kRadialBy], sColRep[kRadialBx], sRowRep[kRadialBy];
     __shared__ int sColN, sRowN;
     const int f = findFrame(tileStart, njobs, blockIdx.x);
     const FrameJob &J = jobs[f];
     const int tile = blockIdx.x - tileStart[f];
-    const int tilesX = (J.W + 31) / 32;
-    const int bx0 = (tile % tilesX) * 32, by0 = (tile / tilesX) * 8;
-    const int ox = bx0 + threadIdx.x, oy = by0 + threadIdx.y;
+    const int tilesX = (J.W + kRadialBx - 1) / kRadialBx;
+    const int bx0 = (tile % tilesX) * kRadialBx, by0 = (tile / tilesX) * kRadialBy;
+    const int ox = bx0 + threadIdx.x;
     const double sx = (double)J.sw / J.W, sy = (double)J.sh / J.H;
     const double widen = fmax(1.0, fmax(sx, sy));
     const float invW = (float)(1.0 / widen);
@@ -1631,7 +1649,7 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
     const int sup = 2 * radius;
     // the block's footprint: first tap of its first pixel to last tap of its
     // last pixel, per axis (the first tap grows with the output index)
-    const int bxLast = min(bx0 + 31, J.W - 1), byLast = min(by0 + 7, J.H - 1);
+    const int bxLast = min(bx0 + kRadialBx - 1, J.W - 1), byLast = min(by0 + kRadialBy - 1, J.H - 1);
     const int fx0 = (int)ceil((bx0 + 0.5) * sx - 0.5 - radius);
     const int fy0 = (int)ceil((by0 + 0.5) * sy - 0.5 - radius);
     const int fw = (int)ceil((bxLast + 0.5) * sx - 0.5 - radius) + sup - fx0;
@@ -1643,24 +1661,20 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
         for (int k = t; k < fw * fh; k += nt)
             sY[k] = (double)ldf(J.Y + (size_t)iclamp(fy0 + k / fw, 0, J.sh - 1) * J.sw +
                                 iclamp(fx0 + k % fw, 0, J.sw - 1));
-    const double cy = (oy + 0.5) * sy - 0.5;
-    const int y0 = (int)ceil(cy - radius);
     const double cx = (ox + 0.5) * sx - 0.5;
     const int x0 = (int)ceil(cx - radius);
     if (grouped && threadIdx.y == 0) {
-        // warp 0: lane l holds column l's offsets and, for l < 8, row l's;
-        // each column (row) joins the group of its first identical predecessor
+        // warp 0: lane l holds column l's offsets and row l's; each column
+        // (row) joins the group of its first identical predecessor
         const int lane = threadIdx.x;
         for (int i = 0; i < sup; ++i)
             sDx[lane][i] = (float)((x0 + i - cx) * invW);
-        if (lane < 8) {
-            const double ry = (by0 + lane + 0.5) * sy - 0.5;
-            const int ry0 = (int)ceil(ry - radius);
-            for (int j = 0; j < sup; ++j)
-                sDy[lane][j] = (float)((ry0 + j - ry) * invW);
-        }
+        const double ry = (by0 + lane + 0.5) * sy - 0.5;
+        const int ry0 = (int)ceil(ry - radius);
+        for (int j = 0; j < sup; ++j)
+            sDy[lane][j] = (float)((ry0 + j - ry) * invW);
         __syncwarp();
-        int c = lane;
+        int c = lane, r = lane;
         for (int q = 0; q < lane && c == lane; ++q) {
             bool same = true;
             for (int i = 0; i < sup && same; ++i)
@@ -1668,30 +1682,24 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
             if (same)
                 c = q;
         }
-        int r = lane;
-        if (lane < 8)
-            for (int q = 0; q < lane && r == lane; ++q) {
-                bool same = true;
-                for (int j = 0; j < sup && same; ++j)
-                    same = __float_as_uint(sDy[q][j]) == __float_as_uint(sDy[lane][j]);
-                if (same)
-                    r = q;
-            }
+        for (int q = 0; q < lane && r == lane; ++q) {
+            bool same = true;
+            for (int j = 0; j < sup && same; ++j)
+                same = __float_as_uint(sDy[q][j]) == __float_as_uint(sDy[lane][j]);
+            if (same)
+                r = q;
+        }
         const unsigned below = (1u << lane) - 1u;
         const unsigned colReps = __ballot_sync(0xffffffffu, c == lane);
-        const unsigned rowReps = __ballot_sync(0xffffffffu, lane < 8 && r == lane);
+        const unsigned rowReps = __ballot_sync(0xffffffffu, r == lane);
         // group number = rank of the representative among the representatives
-        const int myCol = __popc(colReps & below);
+        const int myCol = __popc(colReps & below), myRow = __popc(rowReps & below);
         sColIdx[lane] = __shfl_sync(0xffffffffu, myCol, c);
+        sRowIdx[lane] = __shfl_sync(0xffffffffu, myRow, r);
         if (c == lane)
             sColRep[myCol] = lane;
-        const int myRow = __popc(rowReps & below);
-        const int rowIdx = __shfl_sync(0xffffffffu, myRow, lane < 8 ? r : 0);
-        if (lane < 8) {
-            sRowIdx[lane] = rowIdx;
-            if (r == lane)
-                sRowRep[myRow] = lane;
-        }
+        if (r == lane)
+            sRowRep[myRow] = lane;
         if (lane == 0) {
             sColN = __popc(colReps);
             sRowN = __popc(rowReps);
@@ -1711,42 +1719,51 @@ k_luma_radial(const FrameJob *__restrict__ jobs, const int *__restrict__ tileSta
             }
         __syncthreads();
     }
-    if (ox >= J.W || oy >= J.H)
+    if (ox >= J.W)
         return;
-    double acc = 0.0, wsum = 0.0;
-    if (tabled) {
-        const double *w = sW + (size_t)(sRowIdx[threadIdx.y] * sColN + sColIdx[threadIdx.x]) * sup * sup;
-        const double *s = sY + (y0 - fy0) * fw + (x0 - fx0);
-        if (sup == 6) {
-            radialTabled<6>(w, s, fw, acc, wsum);
-        } else if (sup == 4) {
-            radialTabled<4>(w, s, fw, acc, wsum);
-        } else if (sup == 8) {
-            radialTabled<8>(w, s, fw, acc, wsum);
+    // each thread: the rows threadIdx.y, + 8, + 16, + 24 of its column
+    for (int ly = threadIdx.y; ly < kRadialBy; ly += blockDim.y) {
+        const int oy = by0 + ly;
+        if (oy >= J.H)
+            break;
+        const double cy = (oy + 0.5) * sy - 0.5;
+        const int y0 = (int)ceil(cy - radius);
+        double acc = 0.0, wsum = 0.0;
+        if (tabled) {
+            const double *w = sW + (size_t)(sRowIdx[ly] * sColN + sColIdx[threadIdx.x]) * sup * sup;
+            const double *s = sY + (y0 - fy0) * fw + (x0 - fx0);
+            if (sup == 6) {
+                radialTabled<6>(w, s, fw, acc, wsum);
+            } else if (sup == 4) {
+                radialTabled<4>(w, s, fw, acc, wsum);
+            } else if (sup == 8) {
+                radialTabled<8>(w, s, fw, acc, wsum);
+            } else {
+                for (int j = 0; j < sup; ++j)
+                    for (int i = 0; i < sup; ++i) {
+                        const double wv = w[j * sup + i];
+                        acc = fma(wv, s[j * fw + i], acc);
+                        wsum += wv;
+                    }
+            }
         } else {
-            for (int j = 0; j < sup; ++j)
+            for (int j = 0; j < sup; ++j) {
+                const float dy = (float)((y0 + j - cy) * invW);
+                const int srow = (y0 + j - fy0) * fw - fx0;
+                const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
                 for (int i = 0; i < sup; ++i) {
-                    const double wv = w[j * sup + i];
-                    acc = fma(wv, s[j * fw + i], acc);
-                    wsum += wv;
+                    const float dx = (float)((x0 + i - cx) * invW);
+                    const float w = lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
+                    const double v = tileStaged ? sY[srow + x0 + i]
+                                                : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
+                    acc = fma((double)w, v, acc);
+                    wsum += (double)w;
                 }
-        }
-    } else {
-        for (int j = 0; j < sup; ++j) {
-            const float dy = (float)((y0 + j - cy) * invW);
-            const int srow = (y0 + j - fy0) * fw - fx0;
-            const float *row = J.Y + (size_t)iclamp(y0 + j, 0, J.sh - 1) * J.sw;
-            for (int i = 0; i < sup; ++i) {
-                const float dx = (float)((x0 + i - cx) * invW);
-                const float w = lutLookupDev(J.lut, J.lutN, sqrtf(dx * dx + dy * dy) * J.lutScale);
-                const double v = tileStaged ? sY[srow + x0 + i]
-                                            : (double)ldf(row + iclamp(x0 + i, 0, J.sw - 1));
-                acc = fma((double)w, v, acc);
-                wsum += (double)w;
             }
         }
+        storeLuma(J, ox, oy, (float)(wsum > 1e-6 ? acc / wsum : 0.0));
     }
-    storeLuma(J, ox, oy, (float)(wsum > 1e-6 ? acc / wsum : 0.0));
 }
+
 
 } // namespace lgcr_b200

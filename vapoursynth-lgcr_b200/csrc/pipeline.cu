@@ -925,7 +925,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     }
     switch (s) {
     case S_CONVERT: return convertLumaBlocks(J.sw, J.sh) + convertBlocks(J.cw, J.ch);
-    case S_LUMA_RADIAL: return (resize && J.writeLuma && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
+    case S_LUMA_RADIAL: return (resize && J.writeLuma && J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 32) : 0;
     case S_LUMA_H: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.sh, 8) : 0;
     case S_LUMA_V: return (resize && J.writeLuma && !J.radial) ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_TENSOR: return J.guided ? cdiv(J.sw, kTensorCols * kTensorWarps) * cdiv(J.sh, kTensorRows) : 0;
@@ -1023,25 +1023,28 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     if (plan.totals[S_GUIDED] > 0) {
         // persistent grid: enough resident blocks to fill every SM
         const int variant = plan.cfg.guidedVariant;
-        static int gridBlocks[3] = {0, 0, 0};
+        // the instance with the fused jinc plain base when a frame needs it
+        bool rfuse = false;
+        for (const FrameJob &J : jobs)
+            rfuse = rfuse || radialPlainFused(J);
+        using GuidedKernel = void (*)(const FrameJob *, const int *, int);
+        static const GuidedKernel kernelsOf[2][3] = {
+            {k_guided, k_guided3, k_guided_staged}, {k_guided_r, k_guided3_r, k_guided_staged_r}};
+        const GuidedKernel kern = kernelsOf[rfuse ? 1 : 0][variant];
+        static int gridBlocks[2][3] = {{0, 0, 0}, {0, 0, 0}};
         const size_t dyn = variant == 2 ? kGuidedStageBytes : 0;
-        if (gridBlocks[variant] == 0) {
+        int &grid = gridBlocks[rfuse ? 1 : 0][variant];
+        if (grid == 0) {
             int dev = 0, sms = 0, perSm = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             if (variant == 2)
-                cudaFuncSetAttribute(k_guided_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(kGuidedStageBytes));
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &perSm, variant == 1 ? k_guided3 : variant == 2 ? k_guided_staged : k_guided, 256, dyn);
-            gridBlocks[variant] = std::max(1, sms * std::max(1, perSm));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, 256, dyn);
+            grid = std::max(1, sms * std::max(1, perSm));
         }
-        if (variant == 1)
-            k_guided3<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
-        else if (variant == 2)
-            k_guided_staged<<<gridBlocks[variant], 256, dyn, stream>>>(dJobs, pre(S_GUIDED), n);
-        else
-            k_guided<<<gridBlocks[variant], 256, 0, stream>>>(dJobs, pre(S_GUIDED), n);
+        kern<<<grid, 256, dyn, stream>>>(dJobs, pre(S_GUIDED), n);
         ++launches;
     }
     go(S_YC, k_yc_h, b32x8);

@@ -419,4 +419,14 @@ __device__ __forceinline__ void storeLuma(const FrameJob &J, int x, int y, float
     }
 }
 
+// Jinc selector frames whose guided pass also forms the radial plain base of
+// its listed pixels (pass 1 of the guided pixel): the plain stage skips
+// those pixels and the batch launches the guided kernel instance that has
+// the fused pass (the host decides with this same test).
+__host__ __device__ __forceinline__ bool radialPlainFused(const FrameJob &J) {
+    return J.guided && J.radial && J.algo == 4 && J.rad.valid && J.rad.supX == J.ax.sup &&
+           J.rad.supY == J.ay.sup && J.noClampX && J.noClampY && J.ax.sup == J.ay.sup &&
+           (J.ax.sup == 4 || J.ax.sup == 6 || J.ax.sup == 8);
+}
+
 } // namespace lgcr_b200
