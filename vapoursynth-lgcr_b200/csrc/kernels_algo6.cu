@@ -908,9 +908,24 @@ __global__ void k_blend(LGCR_STAGE_ARGS) {
     const FrameJob &J = jobs[f];
     int ox, oy;
     tile32x8(blockIdx.x - tileStart[f], J.W, ox, oy);
-    if (ox >= J.W || oy >= J.H || !activeOut(J, ox, oy))
+    if (ox >= J.W || oy >= J.H)
         return;
     const size_t o = (size_t)oy * J.W + ox;
+    // final sample: to the typed output when nothing follows the blend
+    auto finish = [&](float u, float v) {
+        if (J.blendStores) {
+            storeChroma(J, 1, ox, oy, u);
+            storeChroma(J, 2, ox, oy, v);
+        } else {
+            J.oU[o] = u;
+            J.oV[o] = v;
+        }
+    };
+    if (!activeOut(J, ox, oy)) {
+        if (J.blendStores)
+            finish(J.oU[o], J.oV[o]);
+        return;
+    }
     const float lam = J.strength4;
     const bool compressed = J.sparse &&
         (unsigned long long)J.counters[kCntActiveOutput] * 2ull < (unsigned long long)J.W * J.H;
@@ -935,14 +950,16 @@ __global__ void k_blend(LGCR_STAGE_ARGS) {
             valueU += w3 * cu * (au * luma + bu - plainU);
             valueV += w3 * cv * (av * luma + bv - plainV);
         }
-        J.oU[o] = valueU;
-        J.oV[o] = valueV;
+        finish(valueU, valueV);
         return;
     }
     const float w2v = J.selW2[o] * lam;
     const float w3v = J.selW3[o] * lam;
-    if (w2v < 1e-4f && w3v < 1e-4f)
+    if (w2v < 1e-4f && w3v < 1e-4f) {
+        if (J.blendStores)
+            finish(plainU, plainV);
         return;
+    }
     const float L0 = bilinearFast(J.Y, J.sw, J.sh, __ldg(J.ax.lbI0 + ox), __ldg(J.ax.lbF + ox),
                                   __ldg(J.ay.lbI0 + oy), __ldg(J.ay.lbF + oy));
     const float au = bilinearFast(J.lgf + 0 * C, cw, ch, cx, cxf, cy, cyf);
@@ -951,8 +968,8 @@ __global__ void k_blend(LGCR_STAGE_ARGS) {
     const float av = bilinearFast(J.lgf + 3 * C, cw, ch, cx, cxf, cy, cyf);
     const float bv = bilinearFast(J.lgf + 4 * C, cw, ch, cx, cxf, cy, cyf);
     const float cv = bilinearFast(J.lgf + 5 * C, cw, ch, cx, cxf, cy, cyf);
-    J.oU[o] = plainU + (w2v * (J.gU[o] - plainU) + w3v * cu * (au * L0 + bu - plainU));
-    J.oV[o] = plainV + (w2v * (J.gV[o] - plainV) + w3v * cv * (av * L0 + bv - plainV));
+    finish(plainU + (w2v * (J.gU[o] - plainU) + w3v * cu * (au * L0 + bu - plainU)),
+           plainV + (w2v * (J.gV[o] - plainV) + w3v * cv * (av * L0 + bv - plainV)));
 }
 
 } // namespace lgcr_b200

@@ -474,6 +474,12 @@ k_plain(LGCR_STAGE_ARGS) {
     const bool table = separable && (J.hTab || fused);
     const bool floatSelector = J.guided && J.algo == 4 && J.outKind == kF32;
     const bool skipListed = J.listed && (!floatSelector || radialPlainFused(J));
+    // every output pixel listed (the trust mask covers the frame) and no
+    // table or extrema for the guided pass to produce here: the guided pass
+    // writes every pixel and nothing here is needed
+    if (skipListed && !J.hTab && !J.wHull && !J.finalInTransfer &&
+        J.counters[kCntActiveOutput] >= (unsigned long long)J.W * J.H)
+        return;
     int syLo = 0, nRows = 0;
     if (table || fused) {
         const int oyLast = oy0 + rowsHere - 1;
