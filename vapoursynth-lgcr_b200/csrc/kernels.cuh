@@ -60,6 +60,7 @@ __global__ void k_count(LGCR_STAGE_ARGS);
 __global__ void k_gate(LGCR_STAGE_ARGS);
 __global__ void k_hpass(LGCR_STAGE_ARGS);
 __global__ void k_plain(LGCR_STAGE_ARGS);
+__global__ void k_plain_all(LGCR_STAGE_ARGS);
 __global__ void k_guided(LGCR_STAGE_ARGS);
 __global__ void k_guided3(LGCR_STAGE_ARGS);
 __global__ void k_guided_staged(LGCR_STAGE_ARGS);

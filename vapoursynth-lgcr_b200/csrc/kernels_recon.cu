@@ -447,8 +447,9 @@ __device__ __forceinline__ void extremaFromRows(const FrameJob &J, const float4 
 // the guided pass lists get their window extrema folded instead (frames
 // with extrema planes), and each warp compacts its remaining plain pixels
 // across its rows so full warps evaluate them.
-__global__ void __launch_bounds__(256, 4)
-k_plain(LGCR_STAGE_ARGS) {
+template <bool EARLY>
+__device__ __forceinline__ void plainStage(const FrameJob *__restrict__ jobs,
+                                           const int *__restrict__ tileStart, int njobs) {
     extern __shared__ __align__(16) unsigned char plainRowsSmem[];
     float2 (*sHV)[32] = reinterpret_cast<float2 (*)[32]>(plainRowsSmem);
     float4 (*sE)[32] = reinterpret_cast<float4 (*)[32]>(      // mnU mxU mnV mxV
@@ -476,8 +477,10 @@ k_plain(LGCR_STAGE_ARGS) {
     const bool skipListed = J.listed && (!floatSelector || radialPlainFused(J));
     // every output pixel listed (the trust mask covers the frame) and no
     // table or extrema for the guided pass to produce here: the guided pass
-    // writes every pixel and nothing here is needed
-    if (skipListed && !J.hTab && !J.wHull && !J.finalInTransfer &&
+    // writes every pixel and nothing here is needed (EARLY instance only:
+    // compiled into the common one, the test costs the separable frames'
+    // plain pass 5 % through its register allocation)
+    if (EARLY && skipListed && !J.hTab && !J.wHull && !J.finalInTransfer &&
         J.counters[kCntActiveOutput] >= (unsigned long long)J.W * J.H)
         return;
     int syLo = 0, nRows = 0;
@@ -673,6 +676,18 @@ k_plain(LGCR_STAGE_ARGS) {
         }
         emit(J, ox, oy, u, v);
     }
+}
+
+__global__ void __launch_bounds__(256, 4)
+k_plain(LGCR_STAGE_ARGS) {
+    plainStage<false>(jobs, tileStart, njobs);
+}
+
+// the instance for launches with jinc selector frames (which often list
+// every output pixel): returns at once for frames the guided pass covers
+__global__ void __launch_bounds__(256, 4)
+k_plain_all(LGCR_STAGE_ARGS) {
+    plainStage<true>(jobs, tileStart, njobs);
 }
 
 // ---------------------------------------------------------------------------

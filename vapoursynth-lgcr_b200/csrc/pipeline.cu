@@ -1010,6 +1010,11 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_GATE, k_gate, b32x8);
     go(S_LGF_DENSE, k_lgf, b32x8);
     go(S_HPASS, k_hpass, b32x8);
+    // jinc selector frames in this launch: the plain and guided instances
+    // that know the guided pass forms their plain base
+    bool rfuse = false;
+    for (const FrameJob &J : jobs)
+        rfuse = rfuse || radialPlainFused(J);
     if (plan.totals[S_PLAIN] > 0) {
         // the dynamic shared-memory opt-in is per device (idempotent, so a
         // race between host threads only repeats it)
@@ -1018,18 +1023,20 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
         cudaGetDevice(&dev);
         if (dev < 0 || dev >= 64 || !plainOptIn[dev].load()) {
             cudaFuncSetAttribute(k_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPlainDynSmem));
+            cudaFuncSetAttribute(k_plain_all, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(kPlainDynSmem));
             if (dev >= 0 && dev < 64)
                 plainOptIn[dev].store(1);
         }
     }
-    go(S_PLAIN, k_plain, b32x8, kPlainDynSmem);
+    if (rfuse)
+        go(S_PLAIN, k_plain_all, b32x8, kPlainDynSmem);
+    else
+        go(S_PLAIN, k_plain, b32x8, kPlainDynSmem);
     if (plan.totals[S_GUIDED] > 0) {
         // persistent grid: enough resident blocks to fill every SM
         const int variant = plan.cfg.guidedVariant;
         // the instance with the fused jinc plain base when a frame needs it
-        bool rfuse = false;
-        for (const FrameJob &J : jobs)
-            rfuse = rfuse || radialPlainFused(J);
         using GuidedKernel = void (*)(const FrameJob *, const int *, int);
         static const GuidedKernel kernelsOf[2][3] = {
             {k_guided, k_guided3, k_guided_staged}, {k_guided_r, k_guided3_r, k_guided_staged_r}};
