@@ -631,6 +631,13 @@ def leg_specs(rank: int):
                      gen={"extra_noise": True}) for i in range(16)],
         filter=dict(algo=2, bm=1, bp=1.0),
         workload="16x1920x1080 YUV420P8 (+noise) -> 4:4:4, algo 2, bm=1, bp=1.0")
+    # where batching pays: frames too small to fill the GPU one at a time
+    legs["small_frames_360p_algo2"] = dict(
+        frames=[dict(width=640, height=360, fmt="420P10", seed=R.frame_seed(12000, rank, i), gen={})
+                for i in range(64)],
+        filter=dict(algo=2, **FILTER_ARGS),
+        workload="64x640x360 YUV420P10 -> 4:4:4, algo 2, lanczos taps=4, sparse=1, qgate=1.0 "
+                 "(not a reference configuration: the batched form's case)")
     return legs
 
 
@@ -937,10 +944,13 @@ def leg_only(args):
         b.run(1)
     torch.cuda.synchronize(dev)
     ms = b.timed(lambda: b.run(1), args.steps)
+    b.per_frame()
+    pms = b.timed(b.per_frame, args.steps)
     stage_ms = b.stage_split(1)
     b.close()
     print(json.dumps({"leg": args.leg, "frames": len(filters), "autotune": tuned,
                       "ms_per_step": round(ms / args.steps, 3),
+                      "per_frame_ms_per_step": round(pms / args.steps, 3),
                       "mpix_s": round(b.out_pixels * args.steps / (ms / 1000) / 1e6, 1),
                       "stage_ms_per_step": {k: round(v, 3) for k, v in
                                             sorted(stage_ms.items(), key=lambda kv: -kv[1])}}))
