@@ -8,7 +8,8 @@
 //                   patch covering it, added in anchor order (the reference's
 //                   sequential += order), then src + 0.65 (filtered - src)
 //                                               src/bm.cpp:393-437
-//   k_backproject   per chroma sample: r = src - mean(2x2 out); out += bp r
+//   k_backproject   per chroma sample: r = src - mean(2x2 out); out += bp r,
+//                   stored to the typed output (the last stage)
 //                                               src/algos.cpp:663-677
 #include "kernels.cuh"
 
@@ -325,6 +326,14 @@ __global__ void k_backproject(LGCR_STAGE_ARGS) {
         const float p01 = o[(size_t)(y0 + 1) * W + x0], p11 = o[(size_t)(y0 + 1) * W + x0 + 1];
         const float r = ldf(srcs[p] + (size_t)cy * J.cw + cx) - 0.25f * (p00 + p10 + p01 + p11);
         const float d = bp * r;
+        if (J.bpStores) {
+            // the last stage: the final samples go to the typed output
+            storeChroma(J, 1 + p, x0, y0, p00 + d);
+            storeChroma(J, 1 + p, x0 + 1, y0, p10 + d);
+            storeChroma(J, 1 + p, x0, y0 + 1, p01 + d);
+            storeChroma(J, 1 + p, x0 + 1, y0 + 1, p11 + d);
+            continue;
+        }
         o[(size_t)y0 * W + x0] = p00 + d;
         o[(size_t)y0 * W + x0 + 1] = p10 + d;
         o[(size_t)(y0 + 1) * W + x0] = p01 + d;

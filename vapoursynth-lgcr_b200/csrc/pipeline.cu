@@ -791,6 +791,9 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     // float algo 4 with nothing after the blend: the blend stores every pixel
     J.blendStores = (J.guided && J.lgfRoiOnly && !J.bm && !J.needBackProject && !J.directOutput)
                         ? 1 : 0;
+    // back-projection is the last stage when it runs, and each output pixel
+    // lies in exactly one chroma sample's 2x2 block: it stores them
+    J.bpStores = J.needBackProject ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -959,7 +962,7 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_BM_AGG: return J.bm ? cdiv(J.W, 32) * cdiv(J.H, 8) : 0;
     case S_BP: return J.needBackProject ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
     case S_LGF_ROI: return (J.guided && J.algo == 4 && J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;
-    case S_STORE: return (J.directOutput || J.finalInTransfer || J.blendStores) ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
+    case S_STORE: return (J.directOutput || J.finalInTransfer || J.blendStores || J.bpStores) ? 0 : cdiv(J.W, 32) * cdiv(J.H, 8);
     }
     return 0;
 }

@@ -159,6 +159,7 @@ struct __align__(16) FrameJob {
     const float *lsXf, *lsYf;
     int lgfRoiOnly;
     int blendStores;                   // the selector blend stores the typed output
+    int bpStores;                      // back-projection stores the typed output
     float *lgf;                        // 6 chroma planes: aU bU confU aV bV confV
     float *selW2, *selW3;              // W x H routing weights (float algo 4)
     float *gU, *gV;                    // W x H guided values (float algo 4)
