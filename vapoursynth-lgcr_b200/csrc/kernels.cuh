@@ -67,6 +67,9 @@ __global__ void k_guided_staged(LGCR_STAGE_ARGS);
 __global__ void k_guided_r(LGCR_STAGE_ARGS);
 __global__ void k_guided3_r(LGCR_STAGE_ARGS);
 __global__ void k_guided_staged_r(LGCR_STAGE_ARGS);
+__global__ void k_guided_o(LGCR_STAGE_ARGS);
+__global__ void k_guided3_o(LGCR_STAGE_ARGS);
+__global__ void k_guided_staged_o(LGCR_STAGE_ARGS);
 // dynamic shared memory of k_guided_staged: 8 warps x 8 x 40 samples of
 // lc (4 B) and the (u, v) pair (16 B)
 constexpr size_t kGuidedStageBytes = size_t(8) * 8 * 40 * (4 + 16);

@@ -995,8 +995,11 @@ struct StagedWindow {
 
 // RFUSE: the kernel instance for batches with jinc selector frames (their
 // pass 1 also forms the plain base); the other instance has no such code, so
-// the separable frames' tap loops keep their schedule.
-template <bool RFUSE>
+// the separable frames' tap loops keep their schedule. RONLY: launches whose
+// frames are all such jinc frames; the separable, extrema-table and
+// temporal paths are compiled out, which leaves the 3-blocks budget far
+// fewer spills.
+template <bool RFUSE, bool RONLY = false>
 __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
                                               const StagedWindow *win) {
     const AxisView &ax = J.ax, &ay = J.ay;
@@ -1098,11 +1101,11 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
         g.havePlain = true;
         g.plainU = (float)v0;
         g.plainV = (float)v1;
-    } else if (J.wHull) {
+    } else if (!RONLY && J.wHull) {
         hMinU = wHull.x; hMaxU = wHull.y; hMinV = wHull.z; hMaxV = wHull.w;
         maxAbsDL = smax(maxAbsDL, fabsf(wLum.y - L0));
         maxAbsDL = smax(maxAbsDL, fabsf(wLum.x - L0));
-    } else if (!J.radial && J.hTab) {
+    } else if (!RONLY && !J.radial && J.hTab) {
         float ext[6];
         switch (ay.sup) {
         case 4: windowExtrema<4>(J, ox, ty0, amy, ext); break;
@@ -1233,7 +1236,7 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     // at the window's luma range maxAbsDL (each rounding step is monotonic),
     // and the frame's bump denominators are bounded on the host.
     const bool rcpSafe = J.bumpRcpSafe && (1.0f + maxAbsDL * maxAbsDL * invSigma2) < kRcpFastLimit;
-    const bool fast = !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
+    const bool fast = !RONLY && !J.radial && J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe;
     // jinc with a phase table: the same unrolled loop with table weights
     const bool fastRadial = J.radial && J.rad.valid && J.rad.supX == ax.sup && J.rad.supY == ay.sup &&
                             J.noClampX && J.noClampY && ax.sup == ay.sup && rcpSafe &&
@@ -1297,7 +1300,7 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
     } else {
         tapsGeneric(J, c, ox, oy, tx0, ty0, a);
     }
-    if (J.tnbCount > 0) {
+    if (!RONLY && J.tnbCount > 0) {
         // TRecon: the neighbours' motion-compensated samples follow the
         // spatial taps in the same accumulators and extend the hull
         TemporalAcc t{a.u, a.v, a.wsum, a.sumAbs, hMinU, hMaxU, hMinV, hMaxV};
@@ -1330,10 +1333,10 @@ __device__ __forceinline__ Guided guidedPixel(const FrameJob &J, int ox, int oy,
 }
 
 // One listed pixel: algo 2 output, or the algo 4 selector (recon.cpp:762-811).
-template <bool RFUSE>
+template <bool RFUSE, bool RONLY>
 __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
                                            const StagedWindow *win) {
-    const Guided g = guidedPixel<RFUSE>(J, ox, oy, win);
+    const Guided g = guidedPixel<RFUSE, RONLY>(J, ox, oy, win);
     if (J.algo == 2) {
         emit(J, ox, oy, (float)g.u, (float)g.v);
         return;
@@ -1434,7 +1437,7 @@ __device__ __forceinline__ void cpAsyncWaitAll() {
 static_assert(kGuidedStageBytes == size_t(8) * kStageRows * kStageCols * (4 + 16),
               "staged guided windows: 8 warps x kStageRows x kStageCols x (lc + (u, v))");
 
-template <int MIN_BLOCKS, bool STAGED, bool RFUSE>
+template <int MIN_BLOCKS, bool STAGED, bool RFUSE, bool RONLY = false>
 __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, int njobs) {
     __shared__ unsigned long long pre[kGuidedMaxFrames + 1];
     extern __shared__ __align__(16) unsigned char guidedStage[];
@@ -1516,7 +1519,7 @@ __device__ __forceinline__ void guidedGrid(const FrameJob *__restrict__ jobs, in
                 }
             }
             if (valid)
-                guidedWork<RFUSE>(J, ox, oy, win);
+                guidedWork<RFUSE, RONLY>(J, ox, oy, win);
             if (STAGED)
                 __syncwarp();                       // the slice is rewritten next round
         }
@@ -1563,6 +1566,25 @@ __global__ void __launch_bounds__(256, 2)
 k_guided_staged_r(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
     (void)tileStart;
     guidedGrid<2, true, true>(jobs, njobs);
+}
+
+// and for launches of jinc selector frames only
+__global__ void __launch_bounds__(256, 2)
+k_guided_o(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2, false, true, true>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 3)
+k_guided3_o(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<3, false, true, true>(jobs, njobs);
+}
+
+__global__ void __launch_bounds__(256, 2)
+k_guided_staged_o(const FrameJob *__restrict__ jobs, const int *__restrict__ tileStart, int njobs) {
+    (void)tileStart;
+    guidedGrid<2, true, true, true>(jobs, njobs);
 }
 
 // Float output planes -> typed output (output conversion stage).

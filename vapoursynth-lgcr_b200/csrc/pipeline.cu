@@ -1015,9 +1015,11 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
     go(S_HPASS, k_hpass, b32x8);
     // jinc selector frames in this launch: the plain and guided instances
     // that know the guided pass forms their plain base
-    bool rfuse = false;
-    for (const FrameJob &J : jobs)
+    bool rfuse = false, ronly = !jobs.empty();
+    for (const FrameJob &J : jobs) {
         rfuse = rfuse || radialPlainFused(J);
+        ronly = ronly && radialPlainFused(J);
+    }
     if (plan.totals[S_PLAIN] > 0) {
         // the dynamic shared-memory opt-in is per device (idempotent, so a
         // race between host threads only repeats it)
@@ -1041,12 +1043,14 @@ int launchStages(const std::vector<FrameJob> &jobs, const StagePlan &plan, const
         const int variant = plan.cfg.guidedVariant;
         // the instance with the fused jinc plain base when a frame needs it
         using GuidedKernel = void (*)(const FrameJob *, const int *, int);
-        static const GuidedKernel kernelsOf[2][3] = {
-            {k_guided, k_guided3, k_guided_staged}, {k_guided_r, k_guided3_r, k_guided_staged_r}};
-        const GuidedKernel kern = kernelsOf[rfuse ? 1 : 0][variant];
-        static int gridBlocks[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        static const GuidedKernel kernelsOf[3][3] = {
+            {k_guided, k_guided3, k_guided_staged}, {k_guided_r, k_guided3_r, k_guided_staged_r},
+            {k_guided_o, k_guided3_o, k_guided_staged_o}};
+        const int inst = ronly ? 2 : rfuse ? 1 : 0;
+        const GuidedKernel kern = kernelsOf[inst][variant];
+        static int gridBlocks[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         const size_t dyn = variant == 2 ? kGuidedStageBytes : 0;
-        int &grid = gridBlocks[rfuse ? 1 : 0][variant];
+        int &grid = gridBlocks[inst][variant];
         if (grid == 0) {
             int dev = 0, sms = 0, perSm = 0;
             cudaGetDevice(&dev);
