@@ -616,21 +616,21 @@ def leg_specs(rank: int):
     on (the headline's 16 1080p frames, all run as algo 2), and the plain,
     jinc-resize and block-refinement configurations."""
     legs = {}
-    legs["north_star_1080p_algo2"] = dict(
+    legs["batched_1080p_p10_algo2"] = dict(
         reuse_headline=True, filter=dict(algo=2, **FILTER_ARGS),
         workload="16x1920x1080 YUV420P10 -> 4:4:4, algo 2, lanczos taps=4, sparse=1, qgate=1.0")
-    legs["config0_720p_p8"] = dict(
+    legs["plain_720p_p8"] = dict(
         frames=[dict(width=1280, height=720, fmt="420P8", seed=R.frame_seed(8000, rank, i), gen={})
                 for i in range(8)],
         filter=dict(algo=2, kernel="lanczos", taps=3, strength=0.8, sigma=0.01),
         workload="8x1280x720 YUV420P8 -> 4:4:4, algo 2, lanczos taps=3, strength 0.8, sigma 0.01")
     for fmt, tag in (("420P16", "p16"), ("420PS", "ps")):
-        legs[f"config2_jinc_resize_{tag}"] = dict(
+        legs[f"jinc_resize_2160p_{tag}"] = dict(
             frames=[dict(width=1920, height=1080, fmt=fmt, seed=R.frame_seed(9000, rank, i),
                          gen={"antialias": True}) for i in range(12)],
             filter=dict(algo=4, kernel="jinc", taps=3, reg=0.005, width=3840, height=2160),
             workload=f"12x1920x1080 YUV{fmt} -> 3840x2160 4:4:4, jinc taps=3, algo 4, reg 0.005")
-    legs["config3_bm_bp"] = dict(
+    legs["bm_bp_1080p_p8"] = dict(
         frames=[dict(width=1920, height=1080, fmt="420P8", seed=R.frame_seed(10000, rank, i),
                      gen={"extra_noise": True}) for i in range(16)],
         filter=dict(algo=2, bm=1, bp=1.0),

@@ -67,8 +67,8 @@ def test_algorithmic_bytes_match_the_formula():
 
 def test_legs_cover_the_other_configurations():
     legs = bench.leg_specs(0)
-    assert set(legs) == {"north_star_1080p_algo2", "config0_720p_p8", "config2_jinc_resize_p16",
-                         "config2_jinc_resize_ps", "config3_bm_bp", "small_frames_360p_algo2"}
-    assert len(legs["config2_jinc_resize_p16"]["frames"]) == 12
+    assert set(legs) == {"batched_1080p_p10_algo2", "plain_720p_p8", "jinc_resize_2160p_p16",
+                         "jinc_resize_2160p_ps", "bm_bp_1080p_p8", "small_frames_360p_algo2"}
+    assert len(legs["jinc_resize_2160p_p16"]["frames"]) == 12
     assert len(legs["small_frames_360p_algo2"]["frames"]) == 64
-    assert legs["config3_bm_bp"]["filter"]["bm"] == 1
+    assert legs["bm_bp_1080p_p8"]["filter"]["bm"] == 1

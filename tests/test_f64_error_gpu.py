@@ -22,22 +22,22 @@ if not O.available("f64"):  # pragma: no cover
     pytest.skip("f64 oracle not built", allow_module_level=True)
 
 CASES = {
-    "config0 720p P8 algo2 lanczos3": (
+    "720p P8 algo2 lanczos3": (
         S.YUV420P8, (1280, 720), dict(seed=1000),
         dict(algo=2, kernel="lanczos", taps=3, strength=0.8, sigma=0.01)),
-    "config1 1080p P10 algo2 lanczos4": (
+    "1080p P10 algo2 lanczos4": (
         S.YUV420P10, (1920, 1080), dict(seed=1002),
         dict(algo=2, kernel="lanczos", taps=4, sparse=1, qgate=1.0)),
-    "config1 1080p P10 algo6 lanczos4": (
+    "1080p P10 algo6 lanczos4": (
         S.YUV420P10, (1920, 1080), dict(seed=1006),
         dict(algo=6, kernel="lanczos", taps=4, sparse=1, qgate=1.0)),
-    "config2 540p->1080p P16 algo4 jinc3": (
+    "540p->1080p P16 algo4 jinc3": (
         S.YUV420P16, (960, 540), dict(seed=2000, antialias=True),
         dict(algo=4, kernel="jinc", taps=3, reg=0.005, width=1920, height=1080)),
-    "config2 540p->1080p PS algo4 jinc3": (
+    "540p->1080p PS algo4 jinc3": (
         S.YUV420PS, (960, 540), dict(seed=2001, antialias=True),
         dict(algo=4, kernel="jinc", taps=3, reg=0.005, width=1920, height=1080)),
-    "config3 1080p P8 algo2 bm bp": (
+    "1080p P8 algo2 bm bp": (
         S.YUV420P8, (1920, 1080), dict(seed=3000, extra_noise=True),
         dict(algo=2, bm=1, bp=1.0)),
 }

@@ -72,13 +72,13 @@ def test_chroma_locations(location):
     assert_parity(got, ref, False, f"location {location}")
 
 
-def test_config0_shape_parity():
-    """1280x720 YUV420P8 algo 2 lanczos3 (benchmark config 0 shape)."""
+def test_720p_p8_lanczos3():
+    """1280x720 YUV420P8 algo 2 lanczos3 (the 720p plain benchmark frame)."""
     fmt = S.YUV420P8
     planes = S.make_frame(1280, 720, fmt, seed=1000)
     got, ref = run_pair(planes, fmt, algo=2, kernel="lanczos", taps=3, strength=0.8,
                         sigma=0.01)
-    assert_parity(got, ref, False, "config0")
+    assert_parity(got, ref, False, "720p P8")
 
 
 @pytest.mark.parametrize("fmt_name", ["420P8", "420P10", "420PS", "422P10", "444PS", "444P8"])
@@ -128,27 +128,27 @@ def test_bm_resize():
 
 
 @pytest.mark.parametrize("algo", [2, 6])
-def test_config1_shape_1080p(algo):
-    """1920x1080 YUV420P10, lanczos4, sparse, qgate 1 (batched config frame)."""
+def test_1080p_p10_lanczos4(algo):
+    """1920x1080 YUV420P10, lanczos4, sparse, qgate 1 (the batched benchmark frame)."""
     fmt = S.YUV420P10
     planes = S.make_frame(1920, 1080, fmt, seed=1000 + algo)
     got, ref = run_pair(planes, fmt, algo=algo, kernel="lanczos", taps=4, sparse=1, qgate=1.0)
-    assert_parity(got, ref, False, f"config1 algo{algo}")
+    assert_parity(got, ref, False, f"1080p P10 algo{algo}")
 
 
 @pytest.mark.parametrize("fmt_name", ["420P16", "420PS"])
-def test_config2_shape_jinc_resize(fmt_name):
-    """960x540 4:2:0 -> 1920x1080 jinc3 algo 4, reg 0.005 (config 2 at half size)."""
+def test_jinc_resize_540p_to_1080p(fmt_name):
+    """960x540 4:2:0 -> 1920x1080 jinc3 algo 4, reg 0.005 (the jinc-resize benchmark at half size)."""
     fmt = FORMATS[fmt_name]
     planes = S.make_frame(960, 540, fmt, seed=2000, antialias=True)
     got, ref = run_pair(planes, fmt, algo=4, kernel="jinc", taps=3, reg=0.005,
                         width=1920, height=1080)
-    assert_parity(got, ref, fmt.is_float, f"config2 {fmt_name}")
+    assert_parity(got, ref, fmt.is_float, f"jinc resize {fmt_name}")
 
 
-def test_config3_shape_bm_bp():
-    """1920x1080 YUV420P8, algo 2, bm, bp 1.0 (config 3 frame)."""
+def test_1080p_p8_bm_bp():
+    """1920x1080 YUV420P8, algo 2, bm, bp 1.0 (the block-refinement benchmark frame)."""
     fmt = S.YUV420P8
     planes = S.make_frame(1920, 1080, fmt, seed=3000, extra_noise=True)
     got, ref = run_pair(planes, fmt, algo=2, bm=1, bp=1.0)
-    assert_parity(got, ref, False, "config3")
+    assert_parity(got, ref, False, "1080p bm bp")
