@@ -11,7 +11,8 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
                HBM, CUDA events on the launching stream, max over ranks
   e2e          same metric through the per-frame C ABI (lgcr_recon_frame) with
                pinned host planes: H2D, run, D2H inside the timed region, one
-               calling host thread per core (at most 16) like fmParallel
+               calling host thread per core (at most 16) like fmParallel,
+               the K steps' frames taken from one continuous queue
                (e2e_pageable: the same with pageable host planes); its
                copy_roofline is the step's H2D/D2H bytes over this box's
                measured duplex pinned-copy rate
@@ -39,6 +40,7 @@ seeded synthetic polygon frames (seed = base + frame index, offset per rank).
 from __future__ import annotations
 
 import argparse
+import collections
 import ctypes
 import json
 import multiprocessing as mp
@@ -1083,16 +1085,20 @@ def our_arm(args):
 
     e2e_threads = args.e2e_threads or min(16, cpu_threads())
 
-    def e2e_pass(nthreads=e2e_threads, ins=pinned_in, outs=pinned_out):
+    def e2e_pass(rounds=1, nthreads=e2e_threads, ins=pinned_in, outs=pinned_out):
+        # `rounds` steps of the workload as one continuous frame queue, the
+        # way a VapourSynth host keeps requesting frames: a thread that
+        # finishes a step's last frame takes the next step's first one
+        # instead of waiting for the slowest thread at a step boundary
         lock = threading.Lock()
-        queue = list(range(len(specs)))
+        queue = collections.deque(i for _ in range(rounds) for i in range(len(specs)))
 
         def worker():
             while True:
                 with lock:
                     if not queue:
                         return
-                    i = queue.pop(0)
+                    i = queue.popleft()
                 f = head_filters[i]
                 t0 = time.perf_counter()
                 f.frame(ins[i], -1, out=outs[i])
@@ -1107,13 +1113,11 @@ def our_arm(args):
 
     # untimed passes grow the per-filter workspace pools to the concurrency
     # the threads reach, so the timed passes allocate nothing
-    for _ in range(max(args.warmup, 1)):
-        e2e_pass()
+    e2e_pass(max(args.warmup, 1))
     latencies.clear()
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_pass()
+    e2e_pass(args.steps)
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - t0
     e2e_s = R.max_over_ranks(e2e_s, dev)
@@ -1127,8 +1131,7 @@ def our_arm(args):
     e2e_pass(ins=page_in, outs=page_out)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_pass(ins=page_in, outs=page_out)
+    e2e_pass(args.steps, ins=page_in, outs=page_out)
     torch.cuda.synchronize(dev)
     e2e_page_s = R.max_over_ranks(time.perf_counter() - t0, dev)
     latencies[:] = e2e_latencies
@@ -1273,7 +1276,7 @@ def main():
     ap.add_argument("--batch-only", action="store_true",
                     help="time the batched form only (profiler captures)")
     ap.add_argument("--no-legs", action="store_true",
-                    help="skip the north-star and per-configuration legs")
+                    help="skip the batched-target and per-workload legs")
     ap.add_argument("--leg", default="",
                     help="run one leg alone (profiler captures): a configuration leg's "
                          "name, sharpen or trecon")
