@@ -480,13 +480,25 @@ k_dilate_v(LGCR_STAGE_ARGS) {
 
 // ---------------------------------------------------------------------------
 // Sparse workset: a block covers 256 consecutive 32-pixel words of the
-// output rows; each warp takes 32 of them in turn, one pixel per lane. An
-// output pixel is active when the mask sample its position maps to is set
-// (every pixel when the frame is not sparse); active pixels mark the 2x2
-// chroma bilinear footprint. The block counts its active pixels, takes one
-// range of the frame's guided work list with one atomic, and the lanes
-// append their pixels (y << 16 | x) in raster order at their prefix offsets.
+// output rows in row-group order (markWord); each warp takes 32 of them in
+// turn, one pixel per lane. An output pixel is active when the mask sample
+// its position maps to is set (every pixel when the frame is not sparse);
+// active pixels mark the 2x2 chroma bilinear footprint. The block counts its
+// active pixels, takes one range of the frame's guided work list with one
+// atomic, and the lanes append their pixels (y << 16 | x) in word order at
+// their prefix offsets.
 // ---------------------------------------------------------------------------
+// Word idx of the frame's list order: groups of G = J.listGroup output
+// rows, a group's words column by column, each column's rows in turn (G = 1:
+// raster order).
+__device__ __forceinline__ void markWord(int idx, int ow, int G, int &oy, int &kw) {
+    G = G < 1 ? 1 : G;
+    const int per = ow * G;
+    const int g = idx / per, rem = idx - g * per;
+    kw = rem / G;
+    oy = g * G + (rem - kw * G);
+}
+
 __device__ __forceinline__ uint32_t activeWord(const FrameJob &J, int kw, int oy) {
     const int x0 = kw * 32;
     const int n = min(32, J.W - x0);
@@ -514,14 +526,13 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
     const int ow = (J.W + 31) / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wordBase = tile * 256 + warp * 32;          // this warp's 32 words
-    // pass 1: lane i counts word wordBase + i
+    // pass 1: lane i counts word wordBase + i (and keeps its position for
+    // pass 2, where the warp walks the words by shuffles)
     uint32_t myBits = 0;
-    {
-        const int idx = wordBase + lane;
-        const int oy = idx / ow, kw = idx - oy * ow;
-        if (oy < J.H)
-            myBits = activeWord(J, kw, oy);
-    }
+    int myOy, myKw;
+    markWord(wordBase + lane, ow, J.listGroup, myOy, myKw);
+    if (myOy < J.H)
+        myBits = activeWord(J, myKw, myOy);
     const unsigned cnt = __popc(myBits);
     unsigned incl = cnt;
     for (int o = 1; o < 32; o <<= 1) {
@@ -550,10 +561,10 @@ k_mark_chroma(LGCR_STAGE_ARGS) {
         const unsigned offs = __shfl_sync(0xffffffffu, excl, i);
         if (!bits)
             continue;                                      // warp-uniform
+        const int oy = __shfl_sync(0xffffffffu, myOy, i);
+        const int kw = __shfl_sync(0xffffffffu, myKw, i);
         if (!((bits >> lane) & 1u))
             continue;
-        const int idx = wordBase + i;
-        const int oy = idx / ow, kw = idx - oy * ow;
         const int ox = kw * 32 + lane;
         if (J.sparse) {
             const int cy0 = __ldg(J.ay.cbI0 + oy);

@@ -1413,8 +1413,9 @@ __device__ __forceinline__ void guidedWork(const FrameJob &J, int ox, int oy,
 // strides over the concatenated work, a warp taking 32 consecutive entries.
 //
 // STAGED: when a warp's 32 pixels are one frame's separable, unclamped fast
-// taps and share their chroma rows (one output row, as the raster-ordered
-// lists mostly give) with at most kStageCols columns between the first and
+// taps and share their chroma rows (one output row, as both list orders
+// mostly give: a warp's 32 entries are one 32-pixel word of one row wherever
+// the frame is dense) with at most kStageCols columns between the first and
 // last window, the warp first copies that window of lc and (u, v) into its
 // shared-memory slice with cp.async (global -> shared, no register round
 // trip); the taps then read shared memory. The values and the arithmetic

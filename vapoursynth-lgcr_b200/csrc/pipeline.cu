@@ -713,6 +713,12 @@ void buildJob(const FrameTask &t, FrameJob &J) {
     J.actList = ws.actList;
     J.listed = J.guided && (p.algo == 2 || p.algo == 4);
     J.xferListed = (J.guided && p.algo == 6 && J.sparse && ws.actList) ? 1 : 0;
+    // upscaling frames (output >= 2x the source luma) list their pixels in row
+    // groups: every chroma sample feeds many output rows there, and a guided
+    // block's pixels then share their windows in L1 (1080p -> 4K jinc guided
+    // pass 9-11 % faster); same-size sparse frames keep the raster order,
+    // whose warps store one row segment each (row groups cost them 1 %)
+    J.listGroup = ((long long)J.W * J.H >= 2LL * J.sw * J.sh) ? kListRowGroup : 1;
     J.chromaList = (J.guided && p.algo == 6 && J.sparse) ? ws.chromaList : nullptr;
     {
         // guided bump denominator 1 + dp^2/g^2 + dt^2/(g*aniso)^2 with aniso >= 1:
@@ -937,7 +943,10 @@ static int stageTilesShaped(const FrameJob &J, int s) {
     case S_TENSOR: return J.guided ? cdiv(J.sw, kTensorCols * kTensorWarps) * cdiv(J.sh, kTensorRows) : 0;
     case S_DIL_H: return J.sparse ? J.sh : 0;
     case S_DIL_V: return J.sparse ? cdiv(J.maskWords, 32) * cdiv(J.sh, 8) : 0;
-    case S_MARK: return (J.sparse || J.listed) ? cdiv(J.H * cdiv(J.W, 32), 256) : 0;
+    case S_MARK: {
+        const int g = std::max(1, J.listGroup);
+        return (J.sparse || J.listed) ? cdiv(cdiv(J.H, g) * g * cdiv(J.W, 32), 256) : 0;
+    }
     case S_COUNT: return J.sparse ? cdiv(J.cw * J.ch, kCountChunk) : 0;
     case S_GATE: return J.useMs ? cdiv(J.cw, 32) * cdiv(J.ch, kGateRows) : 0;
     case S_LGF_DENSE: return (J.guided && J.algo == 4 && !J.lgfRoiOnly) ? cdiv(J.cw, 32) * cdiv(J.ch, 8) : 0;

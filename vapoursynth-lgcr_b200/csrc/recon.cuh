@@ -127,6 +127,7 @@ struct __align__(16) FrameJob {
     double *uvd;                       // cw x ch x 2: (u, v) in FP64
     uint32_t *actList;                 // active output pixels (y << 16 | x)
     int listed;                        // frame uses the guided work list
+    int listGroup;                     // work-list order: output rows per group (1: raster)
     int xferListed;                    // algo 6: detail transfer walks the work list
     uint32_t *chromaList;              // algo 6 sparse: active chroma samples (y << 16 | x)
     int bumpRcpSafe;                   // every guided bump denominator stays below 2^64
