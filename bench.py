@@ -187,6 +187,34 @@ def interleaved(specs):
     return order
 
 
+def frame_queue(n, rounds, nthreads, work, latencies):
+    """Call work(i) for every i in range(n), `rounds` times over, from
+    `nthreads` threads taking the items from one continuous queue -- the way
+    a VapourSynth host keeps requesting frames: a thread that finishes one
+    step's last frame takes the next step's first instead of waiting for the
+    slowest thread at a step boundary. Each call's latency (ms) is appended
+    to `latencies`."""
+    lock = threading.Lock()
+    queue = collections.deque(i for _ in range(rounds) for i in range(n))
+
+    def worker():
+        while True:
+            with lock:
+                if not queue:
+                    return
+                i = queue.popleft()
+            t0 = time.perf_counter()
+            work(i)
+            with lock:
+                latencies.append(1000 * (time.perf_counter() - t0))
+
+    ts = [threading.Thread(target=worker) for _ in range(nthreads)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+
+
 def run_cpu(frames, specs, steps, warmup, threads, per_step, min_seconds=0.0):
     """Each step: `per_step` frames (round-robin over the interleaved
     workload) across `threads` workers, one frame per worker at a time
@@ -1086,30 +1114,8 @@ def our_arm(args):
     e2e_threads = args.e2e_threads or min(16, cpu_threads())
 
     def e2e_pass(rounds=1, nthreads=e2e_threads, ins=pinned_in, outs=pinned_out):
-        # `rounds` steps of the workload as one continuous frame queue, the
-        # way a VapourSynth host keeps requesting frames: a thread that
-        # finishes a step's last frame takes the next step's first one
-        # instead of waiting for the slowest thread at a step boundary
-        lock = threading.Lock()
-        queue = collections.deque(i for _ in range(rounds) for i in range(len(specs)))
-
-        def worker():
-            while True:
-                with lock:
-                    if not queue:
-                        return
-                    i = queue.popleft()
-                f = head_filters[i]
-                t0 = time.perf_counter()
-                f.frame(ins[i], -1, out=outs[i])
-                with lock:
-                    latencies.append(1000 * (time.perf_counter() - t0))
-
-        ts = [threading.Thread(target=worker) for _ in range(nthreads)]
-        for t in ts:
-            t.start()
-        for t in ts:
-            t.join()
+        frame_queue(len(specs), rounds, nthreads,
+                    lambda i: head_filters[i].frame(ins[i], -1, out=outs[i]), latencies)
 
     # untimed passes grow the per-filter workspace pools to the concurrency
     # the threads reach, so the timed passes allocate nothing

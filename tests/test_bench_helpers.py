@@ -72,3 +72,22 @@ def test_legs_cover_the_other_configurations():
     assert len(legs["jinc_resize_2160p_p16"]["frames"]) == 12
     assert len(legs["small_frames_360p_algo2"]["frames"]) == 64
     assert legs["bm_bp_1080p_p8"]["filter"]["bm"] == 1
+
+
+def test_frame_queue_serves_every_frame_once_per_step():
+    import collections
+    import threading
+    calls = collections.Counter()
+    lock = threading.Lock()
+    seen_threads = set()
+
+    def work(i):
+        with lock:
+            calls[i] += 1
+            seen_threads.add(threading.get_ident())
+
+    latencies = []
+    bench.frame_queue(7, 5, 3, work, latencies)
+    assert calls == {i: 5 for i in range(7)}
+    assert len(latencies) == 35 and all(t >= 0.0 for t in latencies)
+    assert 1 <= len(seen_threads) <= 3
